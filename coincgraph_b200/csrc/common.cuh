@@ -1,0 +1,195 @@
+// common.cuh - shared device definitions for libcig (sm_100a).
+//
+// Adjacency layout.  Each vertex owns one power-of-two block of edge slots
+// (at least 4), as the reference's source-local chunk store does
+// (include/groute/graphs/source_local_chunk_store.h:125-145).  Blocks live in
+// an "arena" addressed by a 64-bit edge offset.  The arena is cut into
+// 64 KiB segments (2^14 uint32 slots); a block of 2^c slots with c <= 14 is
+// aligned to its size and therefore never straddles a segment, larger blocks
+// cover whole segments.  The forward arena lives in pinned, mapped host memory
+// (the authoritative copy, read zero-copy) and a device segment table maps a
+// segment either to a 64 KiB slot of the HBM edge cache or to "host".  The
+// reverse arena (in-edges, for deletion repair) is device-only.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cig {
+
+constexpr uint32_t kSegShift = 14;
+constexpr uint64_t kSegEdges = 1ull << kSegShift;
+constexpr uint64_t kSegMask = kSegEdges - 1;
+constexpr uint32_t kMinClass = 2;  // 4-slot minimum block (RequiredChunkCapacity)
+constexpr uint32_t kNumClasses = 40;
+constexpr uint32_t kInf = 0xFFFFFFFFu;
+constexpr uint64_t kInf64 = ~0ull;
+constexpr uint32_t kFull = 0xFFFFFFFFu;
+
+// Device error codes (bit flags in Status::err).
+enum : uint32_t {
+    kErrQueue = 1u << 0,     // a work queue overflowed
+    kErrArena = 1u << 1,     // arena exhausted
+    kErrRounds = 1u << 2,    // round bound exceeded
+    kErrBarrier = 1u << 3,   // grid barrier wait limit exceeded
+    kErrNonFinite = 1u << 4, // PR produced a non-finite value
+    kErrInternal = 1u << 5,
+};
+
+struct RowDesc {
+    uint64_t off;  // first slot of the block in the arena
+    uint32_t deg;  // live entries
+    uint32_t cls;  // block holds 2^cls slots; 0 = no block
+};
+static_assert(sizeof(RowDesc) == 16, "RowDesc must stay 16 bytes");
+
+// Device view of one arena.  For the forward arena `seg_slot` maps segments
+// to cache slots (-1 = host); for a device-only arena it is null and `dev`
+// holds the whole arena.
+struct AdjView {
+    const RowDesc *desc;
+    uint32_t *dev;            // cache pool (forward) or arena (device-only)
+    uint32_t *host;           // mapped host arena (forward) or null
+    const int32_t *seg_slot;  // null for a device-only arena
+
+    __device__ __forceinline__ uint32_t *at(uint64_t off) const {
+        if (!seg_slot) return dev + off;
+        const int32_t s = __ldg(seg_slot + (off >> kSegShift));
+        return s >= 0 ? dev + ((static_cast<uint64_t>(s) << kSegShift) | (off & kSegMask)) : host + off;
+    }
+    __device__ __forceinline__ bool cached(uint64_t off) const {
+        return !seg_slot || __ldg(seg_slot + (off >> kSegShift)) >= 0;
+    }
+    // Writable copies of slot `off`: the authoritative one and, when the
+    // segment is resident, the cached one (write-through).
+    __device__ __forceinline__ void targets(uint64_t off, uint32_t *&primary, uint32_t *&mirror) const {
+        if (!seg_slot) {
+            primary = dev + off;
+            mirror = nullptr;
+            return;
+        }
+        primary = host + off;
+        const int32_t s = seg_slot[off >> kSegShift];
+        mirror = s >= 0 ? dev + ((static_cast<uint64_t>(s) << kSegShift) | (off & kSegMask)) : nullptr;
+    }
+};
+
+struct Status {
+    uint32_t err;
+    uint32_t err_info;
+    uint32_t barrier_count;
+    uint32_t barrier_gen;
+    unsigned long long counters[16];
+};
+
+enum Counter : int {
+    kCntRounds = 0,
+    kCntEdges = 1,
+    kCntEdgesCached = 2,
+    kCntExpanded = 3,
+    kCntAffected = 4,
+    kCntSeeds = 5,
+    kCntMissing = 6,
+    kCntInvalid = 7,
+    kCntChanged = 8,
+    kCntRelocated = 9,
+    kCntSegLoaded = 10,
+    kCntSegEvicted = 11,
+    kCntPrRounds = 12,
+    kCntRemoved = 13,
+};
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__device__ __forceinline__ uint32_t ld_volatile(const uint32_t *p) {
+    return *reinterpret_cast<const volatile uint32_t *>(p);
+}
+
+__device__ __forceinline__ void set_error(Status *st, uint32_t code, uint32_t info = 0) {
+    if ((atomicOr(&st->err, code) & code) == 0) st->err_info = info;
+}
+
+// Warp-aggregated append: one atomicAdd per warp.  All 32 lanes must call.
+__device__ __forceinline__ void warp_enqueue(bool want, uint32_t item, uint32_t *queue, uint32_t *count,
+                                             uint32_t capacity, Status *st) {
+    const uint32_t mask = __ballot_sync(kFull, want);
+    if (!mask) return;
+    const uint32_t lane = lane_id();
+    const uint32_t leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(count, __popc(mask));
+    base = __shfl_sync(kFull, base, leader);
+    if (want) {
+        const uint32_t pos = base + __popc(mask & lanemask_lt());
+        if (pos < capacity)
+            queue[pos] = item;
+        else
+            set_error(st, kErrQueue, pos);
+    }
+}
+
+// Warp-aggregated counter add.
+__device__ __forceinline__ void warp_count(unsigned long long *counter, uint32_t value) {
+    uint32_t sum = __reduce_add_sync(kFull, value);
+    if (lane_id() == 0 && sum) atomicAdd(counter, static_cast<unsigned long long>(sum));
+}
+
+// Grid-wide barrier for cooperatively launched kernels.  Waits are bounded:
+// after ~2 s without progress the waiting block records kErrBarrier and
+// returns false; every later barrier then returns false at once.
+constexpr long long kBarrierTimeoutCycles = 4000000000LL;
+
+__device__ __forceinline__ bool grid_barrier(Status *st) {
+    __syncthreads();
+    __shared__ uint32_t ok;
+    if (threadIdx.x == 0) {
+        ok = 1;
+        const uint32_t gen = atomicAdd(&st->barrier_gen, 0);
+        __threadfence();
+        const uint32_t arrived = atomicAdd(&st->barrier_count, 1);
+        if (arrived == gridDim.x - 1) {
+            atomicExch(&st->barrier_count, 0);
+            __threadfence();
+            atomicAdd(&st->barrier_gen, 1);
+        } else {
+            const long long start = clock64();
+            while (ld_volatile(&st->barrier_gen) == gen) {
+                if (ld_volatile(&st->err) & kErrBarrier) break;
+                if (clock64() - start > kBarrierTimeoutCycles) {
+                    set_error(st, kErrBarrier, blockIdx.x);
+                    break;
+                }
+                __nanosleep(100);
+            }
+        }
+        __threadfence();
+        if (ld_volatile(&st->err) & kErrBarrier) ok = 0;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// Edge weights of the reference samples: BFS 1 (samples/hybrid_bfs/
+// hybrid_bfs.cu:41-47), SSSP (src+dst)%128+1 (include/framework/variants/
+// api.cuh:26-28), CC 0 (samples/hybrid_cc/hybrid_cc.cu:51-57).
+enum Algo : int { kBfs = 0, kSssp = 1, kCc = 2, kPr = 3 };
+
+template <int A>
+__device__ __forceinline__ uint32_t edge_weight(uint32_t u, uint32_t v) {
+    if (A == kBfs) return 1u;
+    if (A == kCc) return 0u;
+    return ((u + v) & 127u) + 1u;  // (u+v) mod 2^32 keeps the residue mod 128
+}
+
+__device__ __forceinline__ uint32_t val_of(unsigned long long s) { return static_cast<uint32_t>(s >> 32); }
+__device__ __forceinline__ uint32_t par_of(unsigned long long s) { return static_cast<uint32_t>(s); }
+__device__ __forceinline__ unsigned long long pack(uint32_t value, uint32_t parent) {
+    return (static_cast<unsigned long long>(value) << 32) | parent;
+}
+
+}  // namespace cig

@@ -1,0 +1,146 @@
+// expand.cuh - load-balanced neighbour-list expansion for one thread block.
+//
+// Every thread of the block brings at most one row (a frontier vertex and its
+// adjacency block).  Rows are served in three tiers so that work per lane
+// stays even whatever the degree mix (scan-based gather, Merrill, Garland and
+// Grimshaw, "Scalable GPU graph traversal", PPoPP 2012):
+//   1. rows with >= TPB entries: the whole block strides over the row;
+//   2. rows with >= 32 entries: the owning warp strides over the row;
+//   3. smaller rows: each warp concatenates its lanes' rows with a warp scan
+//      and hands out the combined edge list 32 entries at a time.
+// The reference balances with CTAWorkSchedulerNew
+// (include/groute/device/cta_scheduler_hybrid.cuh:55-237); this is a new
+// design (tiers, a scan instead of per-row scheduling) that keeps every
+// Op::edge call warp-synchronous so that ops can use warp-aggregated queue
+// appends.
+#pragma once
+
+#include "common.cuh"
+
+namespace cig {
+
+template <int TPB>
+struct ExpandSmem {
+    uint32_t owner;
+    uint32_t b_x, b_payload, b_deg;
+    unsigned long long b_off;
+    uint32_t f_scan[TPB];
+    uint32_t f_x[TPB];
+    uint32_t f_payload[TPB];
+    const uint32_t *f_ptr[TPB];
+};
+
+struct ExpandCounters {
+    uint32_t edges = 0;
+    uint32_t edges_cached = 0;
+    uint32_t rows = 0;
+};
+
+// Op must provide: __device__ void edge(bool valid, uint32_t x, uint32_t payload, uint32_t y) const;
+// edge() is called by all 32 lanes of a warp together (valid=false on padding lanes).
+template <int TPB, class Op>
+__device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint32_t x, uint32_t payload,
+                                            uint64_t off, uint32_t deg, const Op &op, ExpandSmem<TPB> &sm,
+                                            ExpandCounters &cnt) {
+    const uint32_t lane = lane_id();
+    const uint32_t warp = threadIdx.x >> 5;
+    if (has) {
+        cnt.rows += 1;
+        cnt.edges += deg;
+        if (view.cached(off)) cnt.edges_cached += deg;
+    }
+
+    // Tier 1: block-wide rows.  Rows larger than one segment are resolved
+    // per element (view.at), everything else is read from one base pointer.
+    bool big = has && deg >= static_cast<uint32_t>(TPB);
+    while (__syncthreads_or(big)) {
+        if (big) sm.owner = threadIdx.x;
+        __syncthreads();
+        if (sm.owner == threadIdx.x) {
+            sm.b_x = x;
+            sm.b_payload = payload;
+            sm.b_deg = deg;
+            sm.b_off = off;
+            big = false;
+        }
+        __syncthreads();
+        const uint32_t bx = sm.b_x, bp = sm.b_payload, bdeg = sm.b_deg;
+        const uint64_t boff = sm.b_off;
+        if (bdeg <= kSegEdges) {
+            const uint32_t *rp = view.at(boff);
+            for (uint32_t base = 0; base < bdeg; base += TPB) {
+                const uint32_t k = base + threadIdx.x;
+                const bool valid = k < bdeg;
+                const uint32_t y = valid ? __ldg(rp + k) : 0u;
+                op.edge(valid, bx, bp, y);
+            }
+        } else {
+            for (uint32_t base = 0; base < bdeg; base += TPB) {
+                const uint32_t k = base + threadIdx.x;
+                const bool valid = k < bdeg;
+                const uint32_t y = valid ? __ldg(view.at(boff + k)) : 0u;
+                op.edge(valid, bx, bp, y);
+            }
+        }
+        __syncthreads();
+    }
+
+    // Tier 2: warp-wide rows (32 <= deg < TPB, always inside one segment).
+    bool med = has && deg >= 32u && deg < static_cast<uint32_t>(TPB);
+    uint32_t mmask;
+    while ((mmask = __ballot_sync(kFull, med)) != 0u) {
+        const uint32_t leader = __ffs(mmask) - 1;
+        const uint32_t wx = __shfl_sync(kFull, x, leader);
+        const uint32_t wp = __shfl_sync(kFull, payload, leader);
+        const uint32_t wdeg = __shfl_sync(kFull, deg, leader);
+        const uint64_t woff = __shfl_sync(kFull, static_cast<unsigned long long>(off), leader);
+        if (lane == leader) med = false;
+        const uint32_t *rp = view.at(woff);
+        for (uint32_t base = 0; base < wdeg; base += 32u) {
+            const uint32_t k = base + lane;
+            const bool valid = k < wdeg;
+            const uint32_t y = valid ? __ldg(rp + k) : 0u;
+            op.edge(valid, wx, wp, y);
+        }
+    }
+
+    // Tier 3: small rows gathered through a warp scan.
+    const uint32_t mydeg = (has && deg < 32u) ? deg : 0u;
+    uint32_t incl = mydeg;
+#pragma unroll
+    for (uint32_t o = 1; o < 32u; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    if (total == 0) return;
+    const uint32_t wb = warp * 32u;
+    sm.f_scan[wb + lane] = incl - mydeg;
+    sm.f_x[wb + lane] = x;
+    sm.f_payload[wb + lane] = payload;
+    sm.f_ptr[wb + lane] = mydeg ? view.at(off) : nullptr;
+    __syncwarp();
+    for (uint32_t base = 0; base < total; base += 32u) {
+        const uint32_t e = base + lane;
+        const bool valid = e < total;
+        uint32_t ox = 0, op_ = 0, y = 0;
+        if (valid) {
+            // Last lane whose exclusive prefix is <= e owns edge e.
+            uint32_t lo = 0, hi = 32;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (sm.f_scan[wb + mid] <= e)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            ox = sm.f_x[wb + lo];
+            op_ = sm.f_payload[wb + lo];
+            y = __ldg(sm.f_ptr[wb + lo] + (e - sm.f_scan[wb + lo]));
+        }
+        op.edge(valid, ox, op_, y);
+    }
+    __syncwarp();
+}
+
+}  // namespace cig

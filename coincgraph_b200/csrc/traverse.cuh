@@ -1,0 +1,388 @@
+// traverse.cuh - incremental BFS / SSSP / CC kernels.
+//
+// Vertex state is one 64-bit word per vertex: (value << 32) | parent, where
+// value is the BFS depth, SSSP distance or CC label and parent the in-
+// neighbour the value came from.  atomicMin on the packed word updates value
+// and parent together, so a parent is always a witness of its value and ties
+// resolve to the smallest parent id.  The reference keeps value, buffer and
+// parent in three arrays and repairs parents with a CAS loop
+// (samples/hybrid_sssp/hybrid_sssp.cu:110-127); the results it guarantees
+// (unique depths, distances and labels) are the same.
+//
+// Per batch (reference flow: include/framework/framework.cuh:2752-2894 for
+// deletions, :2139-2348 for insertions):
+//   deletion:  seed_deletions -> inval_closure -> reset_affected -> pull_repair
+//              -> enqueue_affected -> push_closure
+//   insertion: seed_insertions -> push_closure
+#pragma once
+
+#include "common.cuh"
+#include "expand.cuh"
+
+namespace cig {
+
+constexpr int kTpb = 256;
+
+// Frontier for the push closure: ping-pong queues and three round counters
+// (round r reads cnt[r%3], appends to cnt[(r+1)%3] and clears cnt[(r+2)%3]).
+struct Frontier {
+    uint32_t *q0;
+    uint32_t *q1;
+    uint32_t *cnt;  // 3 counters
+    uint32_t cap;
+};
+
+// Tag space for per-round queue de-duplication; advanced on the device.
+struct TagState {
+    uint32_t next_tag;
+    uint32_t pad;
+};
+
+// ---------------------------------------------------------------- ops
+
+// Relax x -> y with the value of x (push).  CombineValueBuffer +
+// AccumulateBuffer of the samples (hybrid_sssp.cu:84-127, hybrid_cc.cu:
+// 87-127): improve y, and queue it once per round if its value decreased.
+template <int A>
+struct PushOp {
+    unsigned long long *state;
+    uint32_t *qstamp;
+    uint32_t tag;
+    uint32_t *q_out;
+    uint32_t *q_count;
+    uint32_t q_cap;
+    Status *st;
+
+    __device__ __forceinline__ void edge(bool valid, uint32_t x, uint32_t dx, uint32_t y) const {
+        bool want = false;
+        if (valid) {
+            const uint32_t nd = dx + edge_weight<A>(x, y);
+            const unsigned long long cand = pack(nd, x);
+            if (cand < __ldcg(state + y)) {
+                const unsigned long long old = atomicMin(state + y, cand);
+                if (nd < val_of(old) && __ldcg(qstamp + y) != tag) want = atomicExch(qstamp + y, tag) != tag;
+            }
+        }
+        warp_enqueue(want, y, q_out, q_count, q_cap, st);
+    }
+};
+
+// Deletion dependency of an out-neighbour z of an invalidated vertex x.
+// BFS/SSSP: z's parent is x (IsDeletionDependency, api.cuh:43-49; the packed
+// state makes every parent tight).  CC: equal labels and z is not its own
+// seed (hybrid_cc.cu:45-49), since equal-label cycles may hold parents that
+// do not lead back to the seed.
+template <int A>
+struct InvalOp {
+    unsigned long long *state;
+    uint32_t *aff_stamp;
+    uint32_t epoch;
+    uint32_t *list;   // append base for this round
+    uint32_t *count;  // this round's append counter
+    uint32_t cap;
+    Status *st;
+
+    __device__ __forceinline__ void edge(bool valid, uint32_t x, uint32_t px, uint32_t z) const {
+        bool want = false;
+        if (valid) {
+            const unsigned long long sz = __ldcg(state + z);
+            bool dep;
+            if (A == kCc)
+                dep = z != x && val_of(sz) == px && px < z;
+            else
+                dep = par_of(sz) == x;
+            if (dep && __ldcg(aff_stamp + z) != epoch) want = atomicExch(aff_stamp + z, epoch) != epoch;
+        }
+        warp_enqueue(want, z, list, count, cap, st);
+    }
+};
+
+// Pull over the in-row of an invalidated vertex v (edge u -> v).  Replaces
+// GpuAffectedPullRelax (framework.cuh:137-204): candidates from vertices
+// that kept their value; CC also takes the seed label of invalidated
+// in-neighbours, which are valid reaching ids.
+template <int A>
+struct PullOp {
+    unsigned long long *state;
+    const uint32_t *aff_stamp;
+    uint32_t epoch;
+
+    __device__ __forceinline__ void edge(bool valid, uint32_t v, uint32_t, uint32_t u) const {
+        if (!valid) return;
+        unsigned long long cand;
+        if (__ldcg(aff_stamp + u) == epoch) {
+            if (A != kCc) return;
+            cand = pack(u, u);
+        } else {
+            const uint32_t du = val_of(__ldcg(state + u));
+            if (du == kInf) return;
+            cand = pack(du + edge_weight<A>(u, v), u);
+        }
+        if (cand < __ldcg(state + v)) atomicMin(state + v, cand);
+    }
+};
+
+// ---------------------------------------------------------------- kernels
+
+// Persistent push closure (cooperative launch).  Replaces RunExactGpuClosure
+// (framework.cuh:342-454) and the Start loop (:1151-1182): waves of relaxation
+// until no vertex improves, with bounded grid barriers and a round bound.
+template <int A>
+__global__ void __launch_bounds__(kTpb) push_closure(AdjView fwd, unsigned long long *state, uint32_t *qstamp,
+                                                     TagState *tags, Frontier fr, uint32_t max_rounds,
+                                                     uint32_t *seg_hot, Status *st) {
+    __shared__ ExpandSmem<kTpb> sm;
+    ExpandCounters cnt;
+    // next_tag itself belongs to the seeds queued before this launch.
+    const uint32_t tag0 = tags->next_tag + 1;
+    uint32_t r = 0;
+    for (;; ++r) {
+        const uint32_t n_in = ld_volatile(fr.cnt + (r % 3));
+        if (n_in == 0) break;
+        if (r >= max_rounds) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) set_error(st, kErrRounds, r);
+            break;
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) fr.cnt[(r + 2) % 3] = 0;
+        const uint32_t *in = (r & 1) ? fr.q1 : fr.q0;
+        PushOp<A> op{state, qstamp, tag0 + r, (r & 1) ? fr.q0 : fr.q1, fr.cnt + ((r + 1) % 3), fr.cap, st};
+        for (uint32_t base = blockIdx.x * kTpb; base < n_in; base += gridDim.x * kTpb) {
+            const uint32_t i = base + threadIdx.x;
+            bool has = i < n_in;
+            uint32_t x = 0, dx = 0, deg = 0;
+            uint64_t off = 0;
+            if (has) {
+                x = __ldcg(in + i);
+                dx = val_of(__ldcg(state + x));
+                const RowDesc d = fwd.desc[x];
+                deg = d.deg;
+                off = d.off;
+                has = dx != kInf && deg > 0;
+                if (has && seg_hot) atomicAdd(seg_hot + (off >> kSegShift), 1u);
+            }
+            expand_rows<kTpb>(fwd, has, x, dx, off, deg, op, sm, cnt);
+        }
+        if (!grid_barrier(st)) break;
+    }
+    // Counters (one atomic per warp).
+    warp_count(&st->counters[kCntEdges], cnt.edges);
+    warp_count(&st->counters[kCntEdgesCached], cnt.edges_cached);
+    warp_count(&st->counters[kCntExpanded], cnt.rows);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(&st->counters[kCntRounds], static_cast<unsigned long long>(r));
+        tags->next_tag = tag0 + r + 1;
+    }
+}
+
+// Persistent invalidation closure over the affected list.  Round r processes
+// list[lo, hi) and appends at list[hi + ...] counted by cnt[(r+1)%3].
+// Replaces RunSyncPushDDB_del rounds (framework.cuh:2830-2853).
+template <int A>
+__global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long long *state, uint32_t *aff_stamp,
+                                                      uint32_t epoch, uint32_t *list, uint32_t *cnt3,
+                                                      uint32_t cap, uint32_t max_rounds, uint32_t *aff_total,
+                                                      Status *st) {
+    __shared__ ExpandSmem<kTpb> sm;
+    ExpandCounters c;
+    uint32_t lo = 0, hi = ld_volatile(cnt3 + 0);
+    uint32_t r = 0;
+    for (;; ++r) {
+        if (hi == lo) break;
+        if (r >= max_rounds) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) set_error(st, kErrRounds, r);
+            break;
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) cnt3[(r + 2) % 3] = 0;
+        InvalOp<A> op{state, aff_stamp, epoch, list + hi, cnt3 + ((r + 1) % 3), cap > hi ? cap - hi : 0u, st};
+        const uint32_t n_in = hi - lo;
+        for (uint32_t base = blockIdx.x * kTpb; base < n_in; base += gridDim.x * kTpb) {
+            const uint32_t i = base + threadIdx.x;
+            bool has = i < n_in;
+            uint32_t x = 0, px = 0, deg = 0;
+            uint64_t off = 0;
+            if (has) {
+                x = __ldcg(list + lo + i);
+                px = (A == kCc) ? val_of(__ldcg(state + x)) : x;
+                const RowDesc d = fwd.desc[x];
+                deg = d.deg;
+                off = d.off;
+                has = deg > 0;
+            }
+            expand_rows<kTpb>(fwd, has, x, px, off, deg, op, sm, c);
+        }
+        if (!grid_barrier(st)) break;
+        lo = hi;
+        hi = hi + ld_volatile(cnt3 + ((r + 1) % 3));
+    }
+    warp_count(&st->counters[kCntEdges], c.edges);
+    warp_count(&st->counters[kCntEdgesCached], c.edges_cached);
+    warp_count(&st->counters[kCntExpanded], c.rows);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *aff_total = hi;
+        atomicAdd(&st->counters[kCntRounds], static_cast<unsigned long long>(r));
+        atomicAdd(&st->counters[kCntAffected], static_cast<unsigned long long>(hi));
+    }
+}
+
+// Deletion seeds (reset_del_edges, include/framework/variants/driver.cuh:
+// 371-411), evaluated on the values before the batch.
+template <int A>
+__global__ void seed_deletions(const uint32_t *du, const uint32_t *dv, uint32_t nd, uint32_t n,
+                               const unsigned long long *state, uint32_t *aff_stamp, uint32_t epoch,
+                               uint32_t *list, uint32_t *count, uint32_t cap, Status *st) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool want = false;
+    uint32_t v = 0;
+    if (i < nd) {
+        const uint32_t u = du[i];
+        v = dv[i];
+        if (u < n && v < n) {
+            const unsigned long long sv = __ldcg(state + v);
+            bool dep;
+            if (A == kCc) {
+                const uint32_t lu = val_of(__ldcg(state + u));
+                dep = u != v && lu == val_of(sv) && val_of(sv) < v;
+            } else {
+                dep = par_of(sv) == u && val_of(sv) != kInf;
+            }
+            if (dep && __ldcg(aff_stamp + v) != epoch) want = atomicExch(aff_stamp + v, epoch) != epoch;
+        }
+    }
+    if (__any_sync(kFull, i < nd)) warp_enqueue(want, v, list, count, cap, st);
+}
+
+// value <- initial value for every invalidated vertex (reset_affected_values,
+// driver.cuh:418-433): unreached for BFS/SSSP, its own id for CC.
+template <int A>
+__global__ void reset_affected(const uint32_t *list, const uint32_t *total, unsigned long long *state) {
+    const uint32_t n = *total;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t v = list[i];
+        state[v] = (A == kCc) ? pack(v, kInf) : kInf64;
+    }
+}
+
+template <int A>
+__global__ void __launch_bounds__(kTpb) pull_repair(AdjView rev, unsigned long long *state, const uint32_t *aff_stamp,
+                                                    uint32_t epoch, const uint32_t *list, const uint32_t *total,
+                                                    Status *st) {
+    __shared__ ExpandSmem<kTpb> sm;
+    ExpandCounters c;
+    const uint32_t n = *total;
+    PullOp<A> op{state, aff_stamp, epoch};
+    for (uint32_t base = blockIdx.x * kTpb; base < n; base += gridDim.x * kTpb) {
+        const uint32_t i = base + threadIdx.x;
+        bool has = i < n;
+        uint32_t v = 0, deg = 0;
+        uint64_t off = 0;
+        if (has) {
+            v = list[i];
+            const RowDesc d = rev.desc[v];
+            deg = d.deg;
+            off = d.off;
+            has = deg > 0;
+        }
+        expand_rows<kTpb>(rev, has, v, 0u, off, deg, op, sm, c);
+    }
+    warp_count(&st->counters[kCntEdges], c.edges);
+    warp_count(&st->counters[kCntEdgesCached], c.edges_cached);
+    warp_count(&st->counters[kCntExpanded], c.rows);
+}
+
+// Queue every repaired vertex that has a value (all of them for CC).
+template <int A>
+__global__ void enqueue_affected(const uint32_t *list, const uint32_t *total, const unsigned long long *state,
+                                 Frontier fr, Status *st) {
+    const uint32_t n = *total;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t rounded = (n + 31u) & ~31u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rounded; i += stride) {
+        bool want = false;
+        uint32_t v = 0;
+        if (i < n) {
+            v = list[i];
+            want = (A == kCc) || val_of(__ldcg(state + v)) != kInf;
+        }
+        warp_enqueue(want, v, fr.q0, fr.cnt, fr.cap, st);
+    }
+}
+
+// Insertion seeds (SeedAddedEdgeFrontier, framework.cuh:238-294): relax every
+// inserted edge with the value of its source after the topology update.
+template <int A>
+__global__ void seed_insertions(const uint32_t *au, const uint32_t *av, uint32_t na, uint32_t n,
+                                unsigned long long *state, uint32_t *qstamp, const TagState *tags, Frontier fr,
+                                Status *st) {
+    const uint32_t tag = tags->next_tag;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool want = false;
+    uint32_t v = 0;
+    if (i < na) {
+        const uint32_t u = au[i];
+        v = av[i];
+        if (u < n && v < n) {
+            const uint32_t du = val_of(__ldcg(state + u));
+            if (du != kInf) {
+                const uint32_t nd = du + edge_weight<A>(u, v);
+                const unsigned long long cand = pack(nd, u);
+                if (cand < __ldcg(state + v)) {
+                    const unsigned long long old = atomicMin(state + v, cand);
+                    if (nd < val_of(old)) want = atomicExch(qstamp + v, tag) != tag;
+                }
+            }
+        }
+    }
+    if (__any_sync(kFull, i < na)) warp_enqueue(want, v, fr.q0, fr.cnt, fr.cap, st);
+    if (want) atomicAdd(&st->counters[kCntSeeds], 1ull);
+}
+
+// Static-solve initialisation (InitGraph, framework.cuh:991-1041).
+template <int A>
+__global__ void init_state(unsigned long long *state, uint32_t n, uint32_t source) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        if (A == kCc)
+            state[v] = pack(v, kInf);
+        else
+            state[v] = (v == source) ? pack(0u, kInf) : kInf64;
+    }
+}
+
+// CC starts from every vertex with out-edges.
+__global__ void enqueue_all_nonempty(const RowDesc *desc, uint32_t n, Frontier fr, Status *st) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t rounded = (n + 31u) & ~31u;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < rounded; v += stride) {
+        const bool want = v < n && desc[v].deg > 0;
+        warp_enqueue(want, v, fr.q0, fr.cnt, fr.cap, st);
+    }
+}
+
+__global__ void unpack_values(const unsigned long long *state, uint32_t n, uint32_t *values, uint32_t *parents) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const unsigned long long s = state[v];
+        if (values) values[v] = val_of(s);
+        if (parents) parents[v] = par_of(s);
+    }
+}
+
+// Order-independent 64-bit digest of the values: sum over reached vertices
+// of a SplitMix64 hash of (vertex, value).  Lets a caller confirm a result
+// with 8 bytes over the host link.
+__device__ __forceinline__ unsigned long long digest_mix(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+__global__ void value_digest(const unsigned long long *state, uint32_t n, unsigned long long *out) {
+    unsigned long long acc = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const uint32_t d = val_of(state[v]);
+        if (d != kInf) acc += digest_mix((static_cast<unsigned long long>(v) << 32) | d);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
+    if (lane_id() == 0 && acc) atomicAdd(out, acc);
+}
+
+}  // namespace cig

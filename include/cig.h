@@ -1,0 +1,178 @@
+/*
+ * cig.h - C ABI of libcig, the B200 (sm_100a) incremental streaming-graph engine.
+ *
+ * The reference has no plugin or FFI layer: its boundary is the command line
+ * and text files of four executables (CMakeLists.txt:52-90), built on the
+ * compile-time operator concept AppBase (include/framework/variants/api.cuh:
+ * 22-174) and the Engine methods the samples call.  This header is the thin
+ * C layer under our drop-in hybrid_bfs / hybrid_sssp / hybrid_cc / hybrid_pr
+ * tools; each entry point names the reference interface it replaces.
+ *
+ * Conventions
+ *   - Every function returns 0 on success or a negative cig_status code.
+ *     cig_last_error(h) describes the most recent failure on that handle.
+ *     No C++ exception crosses this boundary.
+ *   - Host pointers passed in are borrowed for the duration of the call.
+ *     Outputs are caller-allocated.  Entry points ending in _device take
+ *     device pointers (CUDA global memory on the handle's device).
+ *   - A handle is used by one host thread at a time; different handles may be
+ *     used concurrently.  After an error reported as CIG_ERR_DEVICE the
+ *     handle's device state is undefined and the handle should be destroyed.
+ *   - Vertex ids are uint32; distances/labels use 0xFFFFFFFF as "unreached".
+ */
+#ifndef CIG_H
+#define CIG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct cig_handle cig_handle;
+
+typedef enum {
+    CIG_OK = 0,
+    CIG_ERR_ARG = -1,       /* invalid argument or call order */
+    CIG_ERR_NOMEM = -2,     /* host or device allocation failed */
+    CIG_ERR_DEVICE = -3,    /* CUDA error */
+    CIG_ERR_ARENA = -4,     /* adjacency arena exhausted */
+    CIG_ERR_LIMIT = -5,     /* a round/iteration bound or a device wait limit was hit */
+    CIG_ERR_STATE = -6,     /* handle unusable after an earlier device error */
+    CIG_ERR_NOTIMPL = -7
+} cig_status;
+
+/* Algorithms of the four reference samples (samples/hybrid_{bfs,sssp,cc,pr}). */
+typedef enum { CIG_BFS = 0, CIG_SSSP = 1, CIG_CC = 2, CIG_PR = 3 } cig_algo;
+
+typedef struct {
+    int32_t algo;            /* cig_algo */
+    int32_t device;          /* CUDA device ordinal */
+    uint32_t source;         /* --source_node (clamped to [0, n-1] at load) */
+    int32_t cache_compat;    /* 1: reference --cache table (include/framework/graph_datum.cuh:158-170) */
+    double cache_gib;        /* --cache: HBM edge-cache budget in GiB of uint32 slots */
+    double pr_epsilon;       /* --error: absolute per-vertex residual threshold */
+    int32_t pr_max_rounds;   /* --pr_max_rounds (1..100 in the reference; any >0 here) */
+    uint32_t max_batch;      /* largest deletion or insertion phase to size buffers for (0: grow) */
+    uint32_t arena_headroom_pct; /* extra arena capacity in percent (0: default 12.5%) */
+    uint32_t flags;          /* CIG_FLAG_* */
+} cig_options;
+
+#define CIG_FLAG_NO_CACHE_REFRESH 0x1u /* keep the segment residency chosen at load */
+#define CIG_FLAG_PR_FP64 0x2u          /* PR ranks/residuals in FP64 (default: FP32 + Kahan) */
+
+typedef struct {
+    uint64_t requested_deletes;
+    uint64_t missing_deletes;    /* as ChunkStoreBatchMetrics::missing_deletes (source_local_chunk_store.h:36-40) */
+    uint64_t requested_additions;
+    uint64_t invalid_additions;  /* out-of-range source or destination */
+    uint64_t changed_sources;
+    uint64_t relocated_rows;     /* rows moved to a larger block */
+    uint64_t affected;           /* vertices invalidated by deletions (BFS/SSSP/CC) */
+    uint64_t seeds;              /* vertices improved directly by inserted edges */
+    uint64_t rounds;             /* traversal rounds (all closures of the batch) */
+    uint64_t edges_scanned;      /* forward + reverse adjacency entries read by traversal */
+    uint64_t edges_scanned_cached; /* of which read from the HBM edge cache or device arena */
+    uint64_t vertices_expanded;
+    uint64_t cache_segments_loaded;
+    uint64_t cache_segments_evicted;
+    double ms_delete;            /* device time of the deletion phase */
+    double ms_insert;            /* device time of the insertion phase */
+    double ms_cache;             /* device time of cache maintenance */
+    uint64_t pr_rounds;
+    double pr_residual_l1;       /* FP64 L1 norm of the PR residual after the batch */
+} cig_batch_stats;
+
+typedef struct {
+    uint32_t n;
+    uint64_t m;
+    uint64_t arena_capacity_edges;
+    uint64_t arena_used_edges;
+    uint64_t segment_edges;
+    uint64_t segments_total;
+    uint64_t segments_resident;
+    uint64_t cache_capacity_segments;
+    uint64_t device_bytes;
+    uint64_t pinned_bytes;
+} cig_graph_info;
+
+/* Fill `o` with the reference's defaults (app_skeleton.h:42-90 and the
+ * per-sample flags). */
+int cig_options_default(cig_options *o);
+
+/* Replaces Engine construction (include/framework/framework.cuh:545-563). */
+int cig_create(const cig_options *o, cig_handle **out);
+int cig_destroy(cig_handle *h);
+const char *cig_last_error(const cig_handle *h);
+
+/* Replaces traversal::Context / ReadGraphMarket_bigdata + LoadGraph
+ * (src/utils/parser.cpp:292-402, include/framework/framework.cuh:800-986):
+ * builds the adjacency from a CSR whose rows are in stored ("file") order. */
+int cig_load_csr(cig_handle *h, uint32_t n, const uint64_t *xadj, const uint32_t *adj);
+
+/* Same, from an edge list in file order (rows keep file order). */
+int cig_load_edges(cig_handle *h, uint32_t n, const uint32_t *src, const uint32_t *dst, uint64_t m);
+
+/* Replaces InitGraph + Start / StartPageRank (framework.cuh:991-1041,
+ * 1151-1182, 1649-1658): the static solve from scratch. */
+int cig_init(cig_handle *h);
+
+/* Replaces del_edge -> update_tree_del (framework.cuh:1564-1586, 2752-2894):
+ * the deletion phase of one batch (topology + incremental repair). */
+int cig_delete_phase(cig_handle *h, const uint32_t *u, const uint32_t *v, uint64_t count,
+                     cig_batch_stats *stats);
+
+/* Replaces add_edge -> update_tree_add (framework.cuh:1397-1401, 2139-2348)
+ * followed by the per-batch cache maintenance (samples/hybrid_sssp/
+ * hybrid_sssp.cu:476-497). */
+int cig_insert_phase(cig_handle *h, const uint32_t *u, const uint32_t *v, uint64_t count,
+                     cig_batch_stats *stats);
+
+/* One whole batch: deletion phase then insertion phase (PR: UpdatePageRank,
+ * framework.cuh:1660-1704).  Host arrays. */
+int cig_apply_batch(cig_handle *h, const uint32_t *del_u, const uint32_t *del_v, uint64_t nd,
+                    const uint32_t *add_u, const uint32_t *add_v, uint64_t na, cig_batch_stats *stats);
+
+/* Same with device-resident arrays. */
+int cig_apply_batch_device(cig_handle *h, const uint32_t *del_u, const uint32_t *del_v, uint64_t nd,
+                           const uint32_t *add_u, const uint32_t *add_v, uint64_t na,
+                           cig_batch_stats *stats);
+
+/* Replaces GatherValue / GatherParent (framework.cuh:2896-2916): BFS depth,
+ * SSSP distance or CC label; parents (0xFFFFFFFF for none). */
+int cig_get_values(cig_handle *h, uint32_t *out);
+int cig_get_parents(cig_handle *h, uint32_t *out);
+
+/* PR ranks and signed residuals (GatherValue/GatherBuffer for hybrid_pr). */
+int cig_get_pr(cig_handle *h, float *rank, float *residual);
+int cig_get_pr64(cig_handle *h, double *rank, double *residual);
+
+/* Order-independent 64-bit digest of the values computed on the device
+ * (sum of a hash of (vertex, value) over reached vertices); 8 bytes cross the
+ * host link.  The reference's ordered DistanceChecksum
+ * (samples/hybrid_sssp/hybrid_sssp.cu:318-330) is computed by the tools on
+ * the host from cig_get_values. */
+int cig_value_digest(cig_handle *h, uint64_t *out);
+
+/* The current adjacency (SourceLocalChunkStore::Descriptor/SlabData views,
+ * source_local_chunk_store.h:395-410): row degrees, one row, or all rows. */
+int cig_num_edges(cig_handle *h, uint64_t *m);
+int cig_get_degrees(cig_handle *h, uint32_t *deg);
+int cig_get_row(cig_handle *h, uint32_t v, uint32_t *out, uint32_t capacity, uint32_t *degree);
+int cig_export_csr(cig_handle *h, uint64_t *xadj, uint32_t *adj);
+
+int cig_graph_info_get(cig_handle *h, cig_graph_info *info);
+
+/* Multi-source queries on the current graph (BASELINE workload 3): k BFS
+ * depths or SSSP distances, k x n row-major, computed with 64-wide bitmask
+ * frontiers.  Does not change the maintained state. */
+int cig_query_bfs_multi(cig_handle *h, const uint32_t *sources, uint32_t k, uint32_t *out_depth);
+int cig_query_sssp_multi(cig_handle *h, const uint32_t *sources, uint32_t k, uint32_t *out_dist);
+
+/* Library version string. */
+const char *cig_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,45 @@
+"""Seeded generator: determinism and the stated properties of its output."""
+import numpy as np
+
+from coincgraph_b200 import gen
+
+
+def test_rmat_deterministic_and_clean(built):
+    a = gen.rmat(10)
+    b = gen.rmat(10)
+    assert np.array_equal(a.xadj, b.xadj) and np.array_equal(a.adj, b.adj)
+    assert a.n == 1024
+    src = np.repeat(np.arange(a.n, dtype=np.uint64), np.diff(a.xadj).astype(np.int64))
+    keys = (src << np.uint64(32)) | a.adj.astype(np.uint64)
+    assert len(np.unique(keys)) == len(keys)  # no duplicates
+    assert not np.any(src == a.adj)  # no self-loops
+    for v in range(0, a.n, 97):
+        row = a.adj[int(a.xadj[v]):int(a.xadj[v + 1])]
+        assert np.all(np.diff(row.astype(np.int64)) > 0)  # rows sorted
+    # id 0 stays the R-MAT hub
+    assert np.argmax(np.diff(a.xadj)) == 0
+
+
+def test_symmetric_graph(built):
+    g = gen.rmat(9, symmetric=True)
+    src = np.repeat(np.arange(g.n, dtype=np.uint64), np.diff(g.xadj).astype(np.int64))
+    fwd = set(((src << np.uint64(32)) | g.adj.astype(np.uint64)).tolist())
+    rev = set(((g.adj.astype(np.uint64) << np.uint64(32)) | src).tolist())
+    assert fwd == rev
+
+
+def test_update_stream_validity(built):
+    g, h = gen.rmat(9, keep_handle=True)
+    ups = gen.updates(h, [50, 50, 50], [40, 40, 40], seed=gen.UPDATE_SEED_BASE + 7)
+    src = np.repeat(np.arange(g.n, dtype=np.uint64), np.diff(g.xadj).astype(np.int64))
+    cur = set(((src << np.uint64(32)) | g.adj.astype(np.uint64)).tolist())
+    for i in range(ups.batches):
+        du, dv, au, av = ups.batch(i)
+        for u, v in zip(du.tolist(), dv.tolist()):
+            assert (u << 32 | v) in cur  # deletions come from the current edge set
+            cur.remove(u << 32 | v)  # without replacement
+        for u, v in zip(au.tolist(), av.tolist()):
+            assert u != v and (u << 32 | v) not in cur  # insertions are new pairs
+            cur.add(u << 32 | v)
+    again = gen.updates(h, [50, 50, 50], [40, 40, 40], seed=gen.UPDATE_SEED_BASE + 7)
+    assert np.array_equal(ups.del_v, again.del_v) and np.array_equal(ups.add_u, again.add_u)

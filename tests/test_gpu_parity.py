@@ -1,0 +1,166 @@
+"""GPU parity: the sm_100a engine (through the C ABI) against the oracle.
+
+Bar: BFS depths, SSSP distances and CC labels bit-exact after the deletion
+phase and after every batch; parents checked as witnesses (they are not
+unique: samples/hybrid_bfs/README.md:7-9); rows equal to the oracle's (and so
+to the reference chunk store's) element for element; missing/invalid counts
+equal.  Cache budgets cover all-resident, mixed residency and zero-copy only.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from coincgraph_b200 import Engine
+from helpers import ORACLE_MODE, adversarial_case, big_row_case, oracle_trace, rmat_case
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+ONE_SEGMENT_GIB = 65536 / 2**30  # one 64 KiB cache slot
+CACHES = {"resident": 4.0, "mixed": ONE_SEGMENT_GIB, "zerocopy": 0.0}
+
+
+def _check_values(eng, g, case, algo, expect, where):
+    got = eng.values()
+    assert np.array_equal(got, expect), f"{algo} values differ {where}: {np.flatnonzero(got != expect)[:10]}"
+    if algo != "cc":
+        mode = ORACLE_MODE[algo]
+        assert g.bellman_check(got, case.source, mode) == (0, 0)
+        assert g.parent_check(got, eng.parents(), case.source, mode)[0] == 0, f"bad parent witness {where}"
+
+
+def run_case(case, algo, cache_gib):
+    trace, _ = oracle_trace(case, algo)
+    g = oracle.Graph(case.n, case.xadj, case.adj)
+    with Engine(algo, source=case.source, cache_gib=cache_gib) as eng:
+        eng.load_csr(case.n, case.xadj, case.adj)
+        eng.init()
+        _check_values(eng, g, case, algo, trace["init"], "after init")
+        for i, (du, dv, au, av) in enumerate(case.batches):
+            missing = g.delete(du, dv)
+            s = eng.delete_phase(du, dv)
+            assert s["missing_deletes"] == missing
+            _check_values(eng, g, case, algo, trace["delete"][i], f"after delete phase {i}")
+            invalid = g.add(au, av)
+            s = eng.insert_phase(au, av)
+            assert s["invalid_additions"] == invalid
+            _check_values(eng, g, case, algo, trace["batch"][i], f"after batch {i}")
+            xadj, adj = eng.export_csr()
+            assert np.array_equal(xadj, trace["rows"][i][0]) and np.array_equal(adj, trace["rows"][i][1])
+
+
+@pytest.mark.parametrize("algo", ["bfs", "sssp", "cc"])
+@pytest.mark.parametrize("cache", list(CACHES))
+def test_rmat_stream(algo, cache):
+    run_case(rmat_case(11, 4, 300, 300, seed_offset=10), algo, CACHES[cache])
+
+
+@pytest.mark.parametrize("algo", ["bfs", "sssp", "cc"])
+def test_adversarial(algo):
+    run_case(adversarial_case(), algo, 4.0)
+
+
+@pytest.mark.parametrize("algo", ["sssp", "cc"])
+@pytest.mark.parametrize("cache", ["resident", "mixed"])
+def test_big_rows(algo, cache):
+    run_case(big_row_case(), algo, CACHES[cache])
+
+
+@pytest.mark.parametrize("algo", ["bfs", "sssp", "cc"])
+def test_symmetric_stream(algo):
+    run_case(rmat_case(10, 3, 200, 200, seed_offset=11, symmetric=True), algo, 4.0)
+
+
+@pytest.mark.parametrize("name", ["rmat8", "adversarial"])
+@pytest.mark.parametrize("algo", ["bfs", "sssp", "cc"])
+def test_golden(name, algo):
+    z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    n, src = int(z["n"]), int(z["source"])
+    with Engine(algo, source=src, cache_gib=4.0) as eng:
+        eng.load_csr(n, z["xadj"], z["adj"])
+        eng.init()
+        assert np.array_equal(eng.values(), z[f"init_{algo}"])
+        for i in range(int(z["nbatches"])):
+            s = eng.delete_phase(z[f"b{i}_du"], z[f"b{i}_dv"])
+            assert s["missing_deletes"] == int(z[f"b{i}_missing"])
+            assert np.array_equal(eng.values(), z[f"b{i}_del_{algo}"])
+            s = eng.insert_phase(z[f"b{i}_au"], z[f"b{i}_av"])
+            assert s["invalid_additions"] == int(z[f"b{i}_invalid"])
+            assert np.array_equal(eng.values(), z[f"b{i}_ins_{algo}"])
+            xadj, adj = eng.export_csr()
+            assert np.array_equal(xadj, z[f"b{i}_xadj"]) and np.array_equal(adj, z[f"b{i}_adj"])
+
+
+@pytest.mark.parametrize("algo", ["bfs", "sssp", "cc"])
+def test_whole_batch_equals_phases(algo):
+    """cig_apply_batch (one sync) gives the same state as the two phase calls."""
+    case = rmat_case(10, 3, 150, 150, seed_offset=12)
+    with Engine(algo, cache_gib=4.0) as a, Engine(algo, cache_gib=4.0) as b:
+        for e in (a, b):
+            e.load_csr(case.n, case.xadj, case.adj)
+            e.init()
+        for du, dv, au, av in case.batches:
+            a.apply_batch(du, dv, au, av)
+            b.delete_phase(du, dv)
+            b.insert_phase(au, av)
+            assert np.array_equal(a.values(), b.values())
+            assert a.digest() == b.digest()
+
+
+def test_device_inputs_match_host_inputs():
+    import torch
+
+    case = rmat_case(11, 2, 400, 400, seed_offset=13)
+    with Engine("sssp", cache_gib=4.0) as a, Engine("sssp", cache_gib=4.0) as b:
+        for e in (a, b):
+            e.load_csr(case.n, case.xadj, case.adj)
+            e.init()
+        for du, dv, au, av in case.batches:
+            a.apply_batch(du, dv, au, av)
+            t = [torch.from_numpy(x.astype(np.int32)).cuda() for x in (du, dv, au, av)]
+            b.apply_batch_device(*t)
+            assert np.array_equal(a.values(), b.values())
+
+
+def test_errors_are_reported():
+    from coincgraph_b200 import CigError
+
+    case = adversarial_case()
+    with Engine("sssp") as eng:
+        with pytest.raises(CigError):
+            eng.init()  # no graph yet
+        eng.load_csr(case.n, case.xadj, case.adj)
+        with pytest.raises(CigError):
+            eng.delete_phase([0], [1])  # before init
+        eng.init()
+        with pytest.raises(CigError):
+            eng.load_csr(case.n, case.xadj, case.adj)  # already loaded
+    with Engine("sssp") as eng:
+        bad = case.adj.copy()
+        bad[0] = case.n + 5
+        with pytest.raises(CigError):
+            eng.load_csr(case.n, case.xadj, bad)
+
+
+def test_arena_exhaustion_is_an_error_not_a_fault():
+    """A tiny arena runs out of room; the call fails cleanly with CIG_ERR_ARENA."""
+    from coincgraph_b200 import CigError
+
+    n = 2048
+    src = np.arange(n, dtype=np.uint32)
+    dst = (src + 1) % n
+    from coincgraph_b200 import gen
+
+    csr = gen.graph_from_edges(n, src, dst)
+    with Engine("bfs", headroom_pct=1) as eng:
+        eng.load_csr(n, csr.xadj, csr.adj)
+        eng.init()
+        rng = np.random.default_rng(3)
+        with pytest.raises(CigError) as err:
+            for _ in range(400):
+                au = rng.integers(0, n, 5000).astype(np.uint32)
+                av = rng.integers(0, n, 5000).astype(np.uint32)
+                eng.apply_batch([], [], au, av)
+        assert err.value.code == -4
