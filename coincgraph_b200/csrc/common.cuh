@@ -45,12 +45,15 @@ static_assert(sizeof(RowDesc) == 16, "RowDesc must stay 16 bytes");
 
 // Device view of one arena.  For the forward arena `seg_slot` maps segments
 // to cache slots (-1 = host); for a device-only arena it is null and `dev`
-// holds the whole arena.
+// holds the whole arena.  The cache is write-back: a resident segment's HBM
+// copy is authoritative and `seg_dirty` marks segments whose host copy is
+// stale (copied back before any host-side read or eviction).
 struct AdjView {
     const RowDesc *desc;
     uint32_t *dev;            // cache pool (forward) or arena (device-only)
     uint32_t *host;           // mapped host arena (forward) or null
     const int32_t *seg_slot;  // null for a device-only arena
+    uint8_t *seg_dirty;       // null for a device-only arena
 
     __device__ __forceinline__ uint32_t *at(uint64_t off) const {
         if (!seg_slot) return dev + off;
@@ -60,17 +63,15 @@ struct AdjView {
     __device__ __forceinline__ bool cached(uint64_t off) const {
         return !seg_slot || __ldg(seg_slot + (off >> kSegShift)) >= 0;
     }
-    // Writable copies of slot `off`: the authoritative one and, when the
-    // segment is resident, the cached one (write-through).
-    __device__ __forceinline__ void targets(uint64_t off, uint32_t *&primary, uint32_t *&mirror) const {
-        if (!seg_slot) {
-            primary = dev + off;
-            mirror = nullptr;
-            return;
-        }
-        primary = host + off;
-        const int32_t s = seg_slot[off >> kSegShift];
-        mirror = s >= 0 ? dev + ((static_cast<uint64_t>(s) << kSegShift) | (off & kSegMask)) : nullptr;
+    // The authoritative copy of slot `off` for writing; marks a resident
+    // segment dirty.  Valid for the whole segment containing `off`.
+    __device__ __forceinline__ uint32_t *wptr(uint64_t off) const {
+        if (!seg_slot) return dev + off;
+        const uint64_t seg = off >> kSegShift;
+        const int32_t s = seg_slot[seg];
+        if (s < 0) return host + off;
+        if (!seg_dirty[seg]) seg_dirty[seg] = 1;
+        return dev + ((static_cast<uint64_t>(s) << kSegShift) | (off & kSegMask));
     }
 };
 
@@ -79,7 +80,7 @@ struct Status {
     uint32_t err_info;
     uint32_t barrier_count;
     uint32_t barrier_gen;
-    unsigned long long counters[16];
+    unsigned long long counters[32];
 };
 
 enum Counter : int {
@@ -97,6 +98,11 @@ enum Counter : int {
     kCntSegEvicted = 11,
     kCntPrRounds = 12,
     kCntRemoved = 13,
+    // Per-kernel groups of 4: edges, edges from HBM, rows expanded, hits.
+    kCntPush = 16,
+    kCntInval = 20,
+    kCntPull = 24,
+    kCntPr = 28,
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }

@@ -182,11 +182,30 @@ struct DevArena {
     uint32_t *host = nullptr;
     uint32_t *host_dptr = nullptr;
     int32_t *seg_slot = nullptr;
+    uint8_t *seg_dirty = nullptr;
     ArenaAlloc *alloc = nullptr;
     uint64_t seg_total = 0;
     uint64_t seg_used = 0;
-    AdjView view() const { return AdjView{desc, dev, host_dptr, seg_slot}; }
+    AdjView view() const { return AdjView{desc, dev, host_dptr, seg_slot, seg_dirty}; }
 };
+
+// Write-back of the edge cache: copy every dirty resident segment to its
+// pinned host copy (one block per segment, 16-byte stores) and clear the flag.
+__global__ void flush_dirty(uint8_t *dirty, const int32_t *seg_slot, const uint32_t *cache, uint32_t *host,
+                            uint64_t nsegs) {
+    for (uint64_t s = blockIdx.x; s < nsegs; s += gridDim.x) {
+        if (!dirty[s]) continue;
+        const int32_t slot = seg_slot[s];
+        if (slot >= 0) {
+            const uint4 *src = reinterpret_cast<const uint4 *>(cache + (static_cast<uint64_t>(slot) << kSegShift));
+            uint4 *dst = reinterpret_cast<uint4 *>(host + (s << kSegShift));
+            for (uint32_t i = threadIdx.x; i < kSegEdges / 4; i += blockDim.x) dst[i] = src[i];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) dirty[s] = 0;
+        __syncthreads();
+    }
+}
 
 const char *kVersion = "cig 0.1.0 (sm_100a)";
 
@@ -241,6 +260,60 @@ struct cig_handle {
     uint32_t *tmp_u32 = nullptr;  // n entries (exports)
     uint64_t last_nd = 0, last_na = 0;
 
+    // Stage profiler (CUDA events on `stream`, resolved in finish()).
+    struct ProfRec {
+        int stage;
+        cudaEvent_t a, b;
+    };
+    bool prof_on = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<ProfRec> prof_pending;
+    cig_stage_profile prof[CIG_STAGE_COUNT] = {};
+
+    cudaEvent_t take_event() {
+        if (ev_used == ev_pool.size()) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            ev_pool.push_back(e);
+        }
+        return ev_pool[ev_used++];
+    }
+    int prof_begin(int stage) {
+        if (!prof_on) return -1;
+        cudaEvent_t a = take_event();
+        CK(cudaEventRecord(a, stream));
+        prof_pending.push_back({stage, a, nullptr});
+        return static_cast<int>(prof_pending.size()) - 1;
+    }
+    void prof_end(int idx) {
+        if (idx < 0) return;
+        cudaEvent_t b = take_event();
+        CK(cudaEventRecord(b, stream));
+        prof_pending[idx].b = b;
+    }
+    void prof_resolve() {
+        for (const auto &p : prof_pending) {
+            float ms = 0;
+            if (p.b && cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+                prof[p.stage].ms += ms;
+                prof[p.stage].launches += 1;
+            }
+        }
+        prof_pending.clear();
+        ev_used = 0;
+        if (!prof_on) return;
+        const unsigned long long *c = h_status->counters;
+        const std::pair<int, int> groups[] = {{CIG_STAGE_PUSH, kCntPush}, {CIG_STAGE_INVAL, kCntInval},
+                                              {CIG_STAGE_PULL, kCntPull}, {CIG_STAGE_PR, kCntPr}};
+        for (const auto &g : groups) {
+            prof[g.first].edges += c[g.second + 0];
+            prof[g.first].edges_cached += c[g.second + 1];
+            prof[g.first].rows += c[g.second + 2];
+            prof[g.first].hits += c[g.second + 3];
+        }
+    }
+
     // ------------------------------------------------------------ helpers
     int grid_for(uint64_t items, int tpb = 256) const {
         const uint64_t g = (items + tpb - 1) / tpb;
@@ -261,6 +334,14 @@ struct cig_handle {
         return per_sm * sms;
     }
 
+    uint64_t n_launch = 0;  // kernels this engine launched (CUB sort kernels not included)
+
+    template <class... P>
+    void launch(void (*kernel)(P...), int grid, int block, typename Identity<P>::type... args) {
+        kernel<<<grid, block, 0, stream>>>(args...);
+        ++n_launch;
+    }
+
     // Arguments are converted to the kernel's exact parameter types, as the
     // void* argument array of a cooperative launch requires.
     template <class... P>
@@ -269,12 +350,16 @@ struct cig_handle {
         const int blocks = coop_blocks(kernel, tpb);
         CK(cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(kernel), dim3(blocks), dim3(tpb), argv, 0,
                                        stream));
+        ++n_launch;
     }
 
     void check_launch() { CK(cudaGetLastError()); }
 
+    uint64_t launch_mark = 0;
+
     void reset_counters() {
         CK(cudaMemsetAsync(status->counters, 0, sizeof(status->counters), stream));
+        launch_mark = n_launch;
     }
 
     void require_alive() const {
@@ -286,6 +371,7 @@ struct cig_handle {
         CK(cudaStreamSynchronize(stream));
         CK(cudaGetLastError());
         CK(cudaMemcpy(h_status, status, sizeof(Status), cudaMemcpyDeviceToHost));
+        prof_resolve();
         const uint32_t e = h_status->err;
         if (e) {
             dead = true;
@@ -342,9 +428,12 @@ struct cig_handle {
         if (stream) cudaStreamSynchronize(stream);
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
+        for (auto &e : ev_pool) cudaEventDestroy(e);
+        ev_pool.clear();
         dfree(fwd.desc);
         dfree(fwd.dev);
         dfree(fwd.seg_slot);
+        dfree(fwd.seg_dirty);
         dfree(fwd.alloc);
         if (fwd.host) cudaFreeHost(fwd.host);
         dfree(rev.desc);
@@ -522,6 +611,8 @@ struct cig_handle {
             for (uint64_t s = 0; s < resident; ++s) slot[s] = static_cast<int32_t>(s);
             dmalloc(fwd.seg_slot, fwd.seg_total);
             CK(cudaMemcpy(fwd.seg_slot, slot.data(), slot.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+            dmalloc(fwd.seg_dirty, fwd.seg_total);
+            CK(cudaMemset(fwd.seg_dirty, 0, fwd.seg_total));
         }
         dmalloc(seg_hot, fwd.seg_total);
         CK(cudaMemset(seg_hot, 0, fwd.seg_total * sizeof(uint32_t)));
@@ -610,12 +701,12 @@ struct cig_handle {
         } else {
             dispatch([&](auto tag) {
                 constexpr int A = decltype(tag)::value;
-                init_state<A><<<persistent_grid(), 256, 0, stream>>>(state, n, source);
+                launch(init_state<A>, persistent_grid(), 256, state, n, source);
                 CK(cudaMemsetAsync(small + kFr, 0, 3 * sizeof(uint32_t), stream));
                 if (A == kCc)
-                    enqueue_all_nonempty<<<persistent_grid(), 256, 0, stream>>>(fwd.desc, n, frontier(), status);
+                    launch(enqueue_all_nonempty, persistent_grid(), 256, fwd.desc, n, frontier(), status);
                 else
-                    set_single<<<1, 1, 0, stream>>>(q0, small + kFr, source);
+                    launch(set_single, 1, 1, q0, small + kFr, source);
                 check_launch();
                 run_push<A>();
             });
@@ -626,7 +717,9 @@ struct cig_handle {
 
     template <int A>
     void run_push() {
+        const int p = prof_begin(CIG_STAGE_PUSH);
         launch_coop(push_closure<A>, kTpb, fwd.view(), state, qstamp, tags, frontier(), n + 2, seg_hot, status);
+        prof_end(p);
     }
 
     // ------------------------------------------------------------ PR
@@ -639,7 +732,7 @@ struct cig_handle {
     template <class T>
     void pr_init_run() {
         auto a = pr_arrays<T>();
-        pr_init<T><<<persistent_grid(), 256, 0, stream>>>(a, n);
+        launch(pr_init<T>, persistent_grid(), 256, a, n);
         const uint32_t counts[3] = {n, 0, 0};
         CK(cudaMemcpyAsync(small + kFr, counts, sizeof(counts), cudaMemcpyHostToDevice, stream));
         check_launch();
@@ -650,12 +743,14 @@ struct cig_handle {
     void pr_run_converge() {
         auto a = pr_arrays<T>();
         const T eps = static_cast<T>(opt.pr_epsilon);
+        const int p = prof_begin(CIG_STAGE_PR);
         launch_coop(pr_converge<T>, kTpbPr, fwd.view(), a, eps, static_cast<uint32_t>(opt.pr_max_rounds), seg_hot,
                     status);
-        pr_normalize_frontier<T><<<persistent_grid(), 256, 0, stream>>>(a);
-        pr_set_counts<T><<<1, 1, 0, stream>>>(a);
+        prof_end(p);
+        launch(pr_normalize_frontier<T>, persistent_grid(), 256, a);
+        launch(pr_set_counts<T>, 1, 1, a);
         CK(cudaMemsetAsync(small64, 0, sizeof(double), stream));
-        pr_residual_l1<T><<<persistent_grid(), 256, 0, stream>>>(static_cast<const T *>(pr_res), n,
+        launch(pr_residual_l1<T>, persistent_grid(), 256, static_cast<const T *>(pr_res), n,
                                                                   reinterpret_cast<double *>(small64));
         check_launch();
     }
@@ -668,23 +763,27 @@ struct cig_handle {
         ++epoch;
         CK(cudaMemsetAsync(small + kTouched, 0, sizeof(uint32_t), stream));
         if (nd + na)
-            collect_touched<<<grid_for(nd + na), 256, 0, stream>>>(d_du, static_cast<uint32_t>(nd), d_au,
+            launch(collect_touched, grid_for(nd + na), 256, d_du, static_cast<uint32_t>(nd), d_au,
                                                                   static_cast<uint32_t>(na), n, aff_stamp, epoch,
                                                                   touched, small + kTouched,
                                                                   static_cast<uint32_t>(2 * bcap), status);
         T *amend = static_cast<T *>(pr_amend);
         // r' = r + alpha (P_new^T - P_old^T) x over the touched sources.
-        pr_amend_contrib<T><<<persistent_grid(), 256, 0, stream>>>(fwd.desc, a, touched, small + kTouched, T(-1),
+        int p = prof_begin(CIG_STAGE_PR);
+        launch(pr_amend_contrib<T>, persistent_grid(), 256, fwd.desc, a, touched, small + kTouched, T(-1),
                                                                    amend);
-        pr_amend_scatter<T><<<persistent_grid(), kTpbPr, 0, stream>>>(fwd.view(), a, touched, small + kTouched,
+        launch(pr_amend_scatter<T>, persistent_grid(), kTpbPr, fwd.view(), a, touched, small + kTouched,
                                                                       amend, eps, status);
+        prof_end(p);
         check_launch();
         mutate_forward_delete(d_du, d_dv, nd, true);
         mutate_forward_add(d_au, d_av, na, true);
-        pr_amend_contrib<T><<<persistent_grid(), 256, 0, stream>>>(fwd.desc, a, touched, small + kTouched, T(1),
+        p = prof_begin(CIG_STAGE_PR);
+        launch(pr_amend_contrib<T>, persistent_grid(), 256, fwd.desc, a, touched, small + kTouched, T(1),
                                                                    amend);
-        pr_amend_scatter<T><<<persistent_grid(), kTpbPr, 0, stream>>>(fwd.view(), a, touched, small + kTouched,
+        launch(pr_amend_scatter<T>, persistent_grid(), kTpbPr, fwd.view(), a, touched, small + kTouched,
                                                                       amend, eps, status);
+        prof_end(p);
         check_launch();
         pr_run_converge<T>();
     }
@@ -708,21 +807,25 @@ struct cig_handle {
         uint32_t *big = forward ? bigf : bigr;
         uint32_t *gcount = small + (forward ? kGcF : kGcR);
         uint32_t *bcount = small + (forward ? kBigF : kBigR);
+        int p = prof_begin(CIG_STAGE_GROUP);
         // make_keys_del fills both kf and kr; only build them once per phase.
         if (forward || opt.algo == CIG_PR) {
-            make_keys_del<<<grid_for(nd), 256, 0, stream>>>(d_du, d_dv, m, n, kf, kr, status);
+            launch(make_keys_del, grid_for(nd), 256, d_du, d_dv, m, n, kf, kr, status);
             check_launch();
         }
         unsigned long long *sorted = sort_keys(keys, tmp, nd);
         CK(cudaMemsetAsync(gcount, 0, sizeof(uint32_t), stream));
         CK(cudaMemsetAsync(bcount, 0, sizeof(uint32_t), stream));
         CK(cudaMemsetAsync(matched, 0, nd * sizeof(uint32_t), stream));
-        find_groups<<<grid_for(nd), 256, 0, stream>>>(sorted, m, groups, gcount);
+        launch(find_groups, grid_for(nd), 256, sorted, m, groups, gcount);
+        prof_end(p);
+        p = prof_begin(forward ? CIG_STAGE_MUTATE : CIG_STAGE_MUTATE_REV);
         unsigned long long *stats = with_stats ? status->counters : nullptr;
-        mutate_delete<<<persistent_grid(), 256, 0, stream>>>(A.view(), A.desc, sorted, m, groups, gcount, matched,
+        launch(mutate_delete, persistent_grid(), 256, A.view(), A.desc, sorted, m, groups, gcount, matched,
                                                              big, bcount, stats, status);
-        mutate_delete_big<<<sms * 2, kTpbMut, 0, stream>>>(A.view(), A.desc, sorted, m, big, bcount, matched,
+        launch(mutate_delete_big, sms * 2, kTpbMut, A.view(), A.desc, sorted, m, big, bcount, matched,
                                                            stats, status);
+        prof_end(p);
         check_launch();
     }
 
@@ -737,22 +840,26 @@ struct cig_handle {
         unsigned long long *plan = forward ? pf : prr;
         uint32_t *gcount = small + (forward ? kGcF : kGcR);
         uint32_t *bcount = small + (forward ? kBigF : kBigR);
+        int p = prof_begin(CIG_STAGE_GROUP);
         if (forward || opt.algo == CIG_PR) {
-            make_keys_add<<<grid_for(na), 256, 0, stream>>>(d_au, d_av, m, n, kf, kr, status);
+            launch(make_keys_add, grid_for(na), 256, d_au, d_av, m, n, kf, kr, status);
             check_launch();
         }
         unsigned long long *sorted = sort_keys(keys, tmp, na);
         CK(cudaMemsetAsync(gcount, 0, sizeof(uint32_t), stream));
         CK(cudaMemsetAsync(bcount, 0, sizeof(uint32_t), stream));
-        find_groups<<<grid_for(na), 256, 0, stream>>>(sorted, m, groups, gcount);
-        plan_add<<<persistent_grid(), 256, 0, stream>>>(A.desc, sorted, m, groups, gcount, plan, A.alloc);
-        alloc_classes<<<1, 64, 0, stream>>>(A.alloc, status);
+        launch(find_groups, grid_for(na), 256, sorted, m, groups, gcount);
+        prof_end(p);
+        p = prof_begin(forward ? CIG_STAGE_MUTATE : CIG_STAGE_MUTATE_REV);
+        launch(plan_add, persistent_grid(), 256, A.desc, sorted, m, groups, gcount, plan, A.alloc);
+        launch(alloc_classes, 1, 64, A.alloc, status);
         unsigned long long *stats = with_stats ? status->counters : nullptr;
         const uint32_t *vals = forward ? d_av : d_au;
-        mutate_add<<<persistent_grid(), 256, 0, stream>>>(A.view(), A.desc, sorted, m, groups, gcount, plan, A.alloc,
+        launch(mutate_add, persistent_grid(), 256, A.view(), A.desc, sorted, m, groups, gcount, plan, A.alloc,
                                                           vals, big, bcount, stats, status);
-        mutate_add_big<<<sms * 2, kTpbMut, 0, stream>>>(A.view(), A.desc, sorted, m, groups, plan, A.alloc, vals, big,
+        launch(mutate_add_big, sms * 2, kTpbMut, A.view(), A.desc, sorted, m, groups, plan, A.alloc, vals, big,
                                                         bcount, stats, status);
+        prof_end(p);
         check_launch();
     }
 
@@ -761,18 +868,24 @@ struct cig_handle {
     void delete_phase_dev(const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd) {
         ++epoch;
         CK(cudaMemsetAsync(small + kFr, 0, 6 * sizeof(uint32_t), stream));  // frontier + affected counters
+        int p = prof_begin(CIG_STAGE_SEED);
         if (nd)
-            seed_deletions<A><<<grid_for(nd), 256, 0, stream>>>(d_du, d_dv, static_cast<uint32_t>(nd), n, state,
+            launch(seed_deletions<A>, grid_for(nd), 256, d_du, d_dv, static_cast<uint32_t>(nd), n, state,
                                                                 aff_stamp, epoch, list, small + kAff, n + 1, status);
+        prof_end(p);
         check_launch();
         mutate_delete_arena(fwd, d_du, d_dv, nd, true, true);
         mutate_delete_arena(rev, d_du, d_dv, nd, false, false);
+        p = prof_begin(CIG_STAGE_INVAL);
         launch_coop(inval_closure<A>, kTpb, fwd.view(), state, aff_stamp, epoch, list, small + kAff, n + 1, n + 2,
                     small + kAffTotal, status);
-        reset_affected<A><<<persistent_grid(), 256, 0, stream>>>(list, small + kAffTotal, state);
-        pull_repair<A><<<persistent_grid(), kTpb, 0, stream>>>(rev.view(), state, aff_stamp, epoch, list,
+        prof_end(p);
+        p = prof_begin(CIG_STAGE_PULL);
+        launch(reset_affected<A>, persistent_grid(), 256, list, small + kAffTotal, state);
+        launch(pull_repair<A>, persistent_grid(), kTpb, rev.view(), state, aff_stamp, epoch, list,
                                                                small + kAffTotal, status);
-        enqueue_affected<A><<<persistent_grid(), 256, 0, stream>>>(list, small + kAffTotal, state, frontier(), status);
+        launch(enqueue_affected<A>, persistent_grid(), 256, list, small + kAffTotal, state, frontier(), status);
+        prof_end(p);
         check_launch();
         run_push<A>();
     }
@@ -782,9 +895,11 @@ struct cig_handle {
         CK(cudaMemsetAsync(small + kFr, 0, 3 * sizeof(uint32_t), stream));
         mutate_add_arena(fwd, d_au, d_av, na, true, true);
         mutate_add_arena(rev, d_au, d_av, na, false, false);
+        int p = prof_begin(CIG_STAGE_SEED);
         if (na)
-            seed_insertions<A><<<grid_for(na), 256, 0, stream>>>(d_au, d_av, static_cast<uint32_t>(na), n, state,
+            launch(seed_insertions<A>, grid_for(na), 256, d_au, d_av, static_cast<uint32_t>(na), n, state,
                                                                  qstamp, tags, frontier(), status);
+        prof_end(p);
         check_launch();
         run_push<A>();
     }
@@ -895,6 +1010,7 @@ struct cig_handle {
         s->cache_segments_loaded = c[kCntSegLoaded];
         s->cache_segments_evicted = c[kCntSegEvicted];
         s->pr_rounds = c[kCntPrRounds];
+        s->kernel_launches = n_launch - launch_mark;
         float ms = 0;
         if (del) {
             cudaEventElapsedTime(&ms, ev[0], ev[1]);
@@ -919,7 +1035,7 @@ struct cig_handle {
     void get_values(uint32_t *out_values, uint32_t *out_parents) {
         require_ready();
         if (opt.algo == CIG_PR) throw CigError(CIG_ERR_ARG, "PageRank has no integer values (cig_get_pr)");
-        unpack_values<<<persistent_grid(), 256, 0, stream>>>(state, n, out_values ? tmp_u32 : nullptr,
+        launch(unpack_values, persistent_grid(), 256, state, n, out_values ? tmp_u32 : nullptr,
                                                               out_parents ? tmp_u32 : nullptr);
         check_launch();
         CK(cudaMemcpyAsync(out_values ? out_values : out_parents, tmp_u32, n * sizeof(uint32_t),
@@ -937,9 +1053,9 @@ struct cig_handle {
         if (rank64) dmalloc(dr64, n);
         if (res64) dmalloc(ds64, n);
         if (pr64)
-            pr_export<double><<<persistent_grid(), 256, 0, stream>>>(pr_arrays<double>(), n, dr, ds, dr64, ds64);
+            launch(pr_export<double>, persistent_grid(), 256, pr_arrays<double>(), n, dr, ds, dr64, ds64);
         else
-            pr_export<float><<<persistent_grid(), 256, 0, stream>>>(pr_arrays<float>(), n, dr, ds, dr64, ds64);
+            launch(pr_export<float>, persistent_grid(), 256, pr_arrays<float>(), n, dr, ds, dr64, ds64);
         check_launch();
         if (rank) CK(cudaMemcpyAsync(rank, dr, n * sizeof(float), cudaMemcpyDeviceToHost, stream));
         if (res) CK(cudaMemcpyAsync(res, ds, n * sizeof(float), cudaMemcpyDeviceToHost, stream));
@@ -956,12 +1072,23 @@ struct cig_handle {
         require_ready();
         if (opt.algo == CIG_PR) throw CigError(CIG_ERR_ARG, "PageRank has no integer values");
         CK(cudaMemsetAsync(small64 + 1, 0, sizeof(unsigned long long), stream));
-        value_digest<<<persistent_grid(), 256, 0, stream>>>(state, n, small64 + 1);
+        launch(value_digest, persistent_grid(), 256, state, n, small64 + 1);
         check_launch();
         unsigned long long h = 0;
         CK(cudaMemcpyAsync(&h, small64 + 1, sizeof(h), cudaMemcpyDeviceToHost, stream));
         CK(cudaStreamSynchronize(stream));
         return h;
+    }
+
+    // Make the pinned host arena current (write back dirty cache segments).
+    void flush_host() {
+        if (!loaded) throw CigError(CIG_ERR_ARG, "load a graph first");
+        require_alive();
+        if (cache_slots) {
+            launch(flush_dirty, sms * 4, 256, fwd.seg_dirty, fwd.seg_slot, fwd.dev, fwd.host_dptr, fwd.seg_total);
+            check_launch();
+        }
+        CK(cudaStreamSynchronize(stream));
     }
 
     std::vector<RowDesc> host_desc() {
@@ -1140,7 +1267,7 @@ int cig_get_row(cig_handle *h, uint32_t v, uint32_t *out, uint32_t capacity, uin
         if (!h->loaded) throw CigError(CIG_ERR_ARG, "load a graph first");
         if (v >= h->n) throw CigError(CIG_ERR_ARG, "vertex out of range");
         RowDesc d;
-        CK(cudaStreamSynchronize(h->stream));
+        h->flush_host();
         CK(cudaMemcpy(&d, h->fwd.desc + v, sizeof(d), cudaMemcpyDeviceToHost));
         if (degree) *degree = d.deg;
         if (out) std::memcpy(out, h->fwd.host + d.off, std::min(capacity, d.deg) * sizeof(uint32_t));
@@ -1154,6 +1281,7 @@ int cig_export_csr(cig_handle *h, uint64_t *xadj, uint32_t *adj) {
         xadj[0] = 0;
         for (uint32_t v = 0; v < h->n; ++v) xadj[v + 1] = xadj[v] + d[v].deg;
         if (!adj) return;
+        h->flush_host();
         const uint32_t *arena = h->fwd.host;
         parallel_for(h->n, [&](uint64_t b, uint64_t e) {
             for (uint64_t v = b; v < e; ++v)
@@ -1184,6 +1312,23 @@ int cig_graph_info_get(cig_handle *h, cig_graph_info *info) {
         cudaMemGetInfo(&free_b, &total_b);
         info->device_bytes = total_b - free_b;
         info->pinned_bytes = h->fwd.seg_total * kSegEdges * sizeof(uint32_t);
+    });
+}
+
+int cig_profile_enable(cig_handle *h, int enable) {
+    return guarded(h, [&] {
+        CK(cudaStreamSynchronize(h->stream));
+        h->prof_pending.clear();
+        h->ev_used = 0;
+        std::memset(h->prof, 0, sizeof(h->prof));
+        h->prof_on = enable != 0;
+    });
+}
+
+int cig_profile_read(cig_handle *h, cig_stage_profile *out, uint32_t count) {
+    return guarded(h, [&] {
+        if (!out) throw CigError(CIG_ERR_ARG, "null output");
+        std::memcpy(out, h->prof, std::min<uint32_t>(count, CIG_STAGE_COUNT) * sizeof(cig_stage_profile));
     });
 }
 

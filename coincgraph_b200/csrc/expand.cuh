@@ -34,9 +34,23 @@ struct ExpandCounters {
     uint32_t edges = 0;
     uint32_t edges_cached = 0;
     uint32_t rows = 0;
+    uint32_t hits = 0;  // edges whose op changed state (relaxations, claims)
 };
 
-// Op must provide: __device__ void edge(bool valid, uint32_t x, uint32_t payload, uint32_t y) const;
+// Add a thread's counters to the batch totals and to one kernel's group of
+// four slots (edges, edges served from HBM, rows, hits).  All lanes call.
+__device__ __forceinline__ void flush_counters(Status *st, const ExpandCounters &c, int group) {
+    warp_count(&st->counters[kCntEdges], c.edges);
+    warp_count(&st->counters[kCntEdgesCached], c.edges_cached);
+    warp_count(&st->counters[kCntExpanded], c.rows);
+    warp_count(&st->counters[group + 0], c.edges);
+    warp_count(&st->counters[group + 1], c.edges_cached);
+    warp_count(&st->counters[group + 2], c.rows);
+    warp_count(&st->counters[group + 3], c.hits);
+}
+
+// Op must provide: __device__ bool edge(bool valid, uint32_t x, uint32_t payload, uint32_t y) const;
+// returning true when the edge changed state.
 // edge() is called by all 32 lanes of a warp together (valid=false on padding lanes).
 template <int TPB, class Op>
 __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint32_t x, uint32_t payload,
@@ -72,14 +86,14 @@ __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint3
                 const uint32_t k = base + threadIdx.x;
                 const bool valid = k < bdeg;
                 const uint32_t y = valid ? __ldg(rp + k) : 0u;
-                op.edge(valid, bx, bp, y);
+                cnt.hits += op.edge(valid, bx, bp, y);
             }
         } else {
             for (uint32_t base = 0; base < bdeg; base += TPB) {
                 const uint32_t k = base + threadIdx.x;
                 const bool valid = k < bdeg;
                 const uint32_t y = valid ? __ldg(view.at(boff + k)) : 0u;
-                op.edge(valid, bx, bp, y);
+                cnt.hits += op.edge(valid, bx, bp, y);
             }
         }
         __syncthreads();
@@ -100,7 +114,7 @@ __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint3
             const uint32_t k = base + lane;
             const bool valid = k < wdeg;
             const uint32_t y = valid ? __ldg(rp + k) : 0u;
-            op.edge(valid, wx, wp, y);
+            cnt.hits += op.edge(valid, wx, wp, y);
         }
     }
 
@@ -138,7 +152,7 @@ __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint3
             op_ = sm.f_payload[wb + lo];
             y = __ldg(sm.f_ptr[wb + lo] + (e - sm.f_scan[wb + lo]));
         }
-        op.edge(valid, ox, op_, y);
+        cnt.hits += op.edge(valid, ox, op_, y);
     }
     __syncwarp();
 }

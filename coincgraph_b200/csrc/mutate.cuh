@@ -146,17 +146,143 @@ __device__ __forceinline__ bool find_run(const unsigned long long *keys, uint32_
 }
 
 __device__ __forceinline__ void write_slot(const AdjView &view, unsigned long long off, uint32_t value) {
-    uint32_t *p, *mirror;
-    view.targets(off, p, mirror);
-    *p = value;
-    if (mirror) *mirror = value;
+    *view.wptr(off) = value;
+}
+
+// Compact one 128-entry chunk of a row in place, given per-element keep
+// flags for the 4 consecutive elements each lane holds (positions
+// base + 4*lane + s).  The survivors are staged in shared memory and written
+// back with coalesced stores; nothing is written while no entry at or before
+// this chunk was deleted.  All 32 lanes call.
+__device__ __forceinline__ uint32_t warp_compact4(uint32_t *dst, uint32_t *stage, uint32_t w, uint32_t base,
+                                                  const uint32_t (&e)[4], const bool (&keep)[4], uint32_t valid) {
+    const uint32_t lane = lane_id();
+    const uint32_t kc = keep[0] + keep[1] + keep[2] + keep[3];
+    uint32_t incl = kc;
+#pragma unroll
+    for (uint32_t o = 1; o < 32u; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    if (w == base && total == valid) return w + total;  // nothing moved yet
+    uint32_t pos = incl - kc;
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+        if (keep[s]) stage[pos++] = e[s];
+    __syncwarp();
+    for (uint32_t i = lane; i < total; i += 32u) dst[w + i] = stage[i];
+    __syncwarp();
+    return w + total;
+}
+
+// Deletion of a group with at most 32 runs' keys: the destinations live in
+// lane registers (lane j holds key j), matched counts in the run-head lanes.
+// The row lies inside one segment (deg <= kWarpRowMax).
+__device__ __forceinline__ uint32_t warp_delete_regs(const AdjView &view, const RowDesc &d,
+                                                     const unsigned long long *keys, uint32_t gs, uint32_t m,
+                                                     uint32_t *stage) {
+    const uint32_t lane = lane_id();
+    const bool kvalid = lane < m;
+    const uint32_t kd = kvalid ? key_low(keys[gs + lane]) : 0u;
+    const uint32_t vmask = __ballot_sync(kFull, kvalid);
+    uint32_t peers = __match_any_sync(kFull, kd) & vmask;
+    const uint32_t req_here = kvalid ? __popc(peers) : 0u;  // multiplicity of this lane's run
+    uint32_t mcount = 0;                                     // matched so far (run-head lanes)
+    const uint32_t *src = view.at(d.off);
+    uint32_t *dst = nullptr;  // resolved (and the segment marked dirty) on the first move
+    uint32_t w = 0;
+    for (uint32_t base = 0; base < d.deg; base += 128u) {
+        const uint32_t k0 = base + 4u * lane;
+        uint32_t e[4] = {0, 0, 0, 0};
+        if (k0 < d.deg) {
+            const uint4 q = *reinterpret_cast<const uint4 *>(src + k0);
+            e[0] = q.x;
+            e[1] = q.y;
+            e[2] = q.z;
+            e[3] = q.w;
+        }
+        int run[4] = {-1, -1, -1, -1};
+        for (uint32_t j = 0; j < m; ++j) {
+            const uint32_t kj = __shfl_sync(kFull, kd, j);
+#pragma unroll
+            for (int s = 0; s < 4; ++s)
+                if (run[s] < 0 && k0 + s < d.deg && e[s] == kj) run[s] = static_cast<int>(j);
+        }
+        bool del[4] = {false, false, false, false};
+        uint32_t cm[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) cm[s] = __ballot_sync(kFull, run[s] >= 0);
+        uint32_t any = cm[0] | cm[1] | cm[2] | cm[3];
+        // Resolve candidates in position order (lane-major, then s).
+        while (any) {
+            const uint32_t l = __ffs(any) - 1;
+            any &= any - 1;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                if ((cm[s] >> l) & 1u) {
+                    const uint32_t r = static_cast<uint32_t>(__shfl_sync(kFull, run[s], l));
+                    const uint32_t req = __shfl_sync(kFull, req_here, r);
+                    const uint32_t seen = __shfl_sync(kFull, mcount, r);
+                    if (lane == r) mcount = seen + 1;
+                    if (lane == l) del[s] = seen < req;
+                }
+            }
+        }
+        bool keep[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) keep[s] = (k0 + s < d.deg) && !del[s];
+        const uint32_t valid = min(128u, d.deg - base);
+        if (!dst && (cm[0] | cm[1] | cm[2] | cm[3] | (w != base))) dst = view.wptr(d.off);
+        w = warp_compact4(dst, stage, w, base, e, keep, valid);
+    }
+    return w;
+}
+
+// Generic warp deletion (any number of keys): binary search in the sorted
+// group keys in global memory, `matched[run]` counts occurrences seen.
+__device__ __forceinline__ uint32_t warp_delete_global(const AdjView &view, const RowDesc &d, uint32_t u,
+                                                       const unsigned long long *keys, uint32_t gs, uint32_t ge,
+                                                       uint32_t *matched) {
+    const uint32_t lane = lane_id();
+    const unsigned long long uhi = static_cast<unsigned long long>(u) << kKeyShift;
+    uint32_t w = 0;
+    for (uint32_t base = 0; base < d.deg; base += 32u) {
+        const uint32_t k = base + lane;
+        const bool valid = k < d.deg;
+        const uint32_t x = valid ? *view.at(d.off + k) : 0u;
+        uint32_t run = 0xFFFFFFFFu, req = 0;
+        const bool cand = valid && find_run(keys, gs, ge, uhi | x, run, req);
+        bool del = false;
+        if (__ballot_sync(kFull, cand)) {
+            const uint32_t peers = __match_any_sync(kFull, run);
+            const uint32_t before = __popc(peers & lanemask_lt());
+            uint32_t seen = 0;
+            if (cand) seen = matched[run];
+            del = cand && seen + before < req;
+            __syncwarp();
+            if (cand && before == 0) matched[run] = seen + __popc(peers);
+            __syncwarp();
+        }
+        const bool keep = valid && !del;
+        const uint32_t km = __ballot_sync(kFull, keep);
+        const uint32_t pos = w + __popc(km & lanemask_lt());
+        __syncwarp();
+        if (keep && pos != k) write_slot(view, d.off + pos, x);
+        w += __popc(km);
+    }
+    return w;
 }
 
 // Deletion phase, one warp per source group; rows above kWarpRowMax go to
-// the block path.  `matched[run]` counts occurrences of a run already seen.
-__global__ void mutate_delete(AdjView view, RowDesc *desc, const unsigned long long *keys, uint32_t m,
+// the block path.  Launched with kMutWarps * 32 threads per block.
+constexpr int kMutWarps = 8;
+
+__global__ void __launch_bounds__(kMutWarps * 32) mutate_delete(AdjView view, RowDesc *desc, const unsigned long long *keys, uint32_t m,
                               const uint32_t *groups, const uint32_t *gcount, uint32_t *matched, uint32_t *big,
                               uint32_t *big_count, unsigned long long *stats, Status *st) {
+    __shared__ uint32_t stage_all[kMutWarps][128];
+    uint32_t *stage = stage_all[threadIdx.x >> 5];
     const uint32_t lane = lane_id();
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t ng = *gcount;
@@ -170,32 +296,8 @@ __global__ void mutate_delete(AdjView view, RowDesc *desc, const unsigned long l
             if (lane == 0) big[atomicAdd(big_count, 1u)] = gs;
             continue;
         }
-        const unsigned long long uhi = static_cast<unsigned long long>(u) << kKeyShift;
-        uint32_t w = 0;
-        for (uint32_t base = 0; base < d.deg; base += 32u) {
-            const uint32_t k = base + lane;
-            const bool valid = k < d.deg;
-            const uint32_t x = valid ? *view.at(d.off + k) : 0u;
-            uint32_t run = 0xFFFFFFFFu, req = 0;
-            const bool cand = valid && find_run(keys, gs, ge, uhi | x, run, req);
-            bool del = false;
-            if (__ballot_sync(kFull, cand)) {
-                const uint32_t peers = __match_any_sync(kFull, run);
-                const uint32_t before = __popc(peers & lanemask_lt());
-                uint32_t seen = 0;
-                if (cand) seen = matched[run];
-                del = cand && seen + before < req;
-                __syncwarp();
-                if (cand && before == 0) matched[run] = seen + __popc(peers);
-                __syncwarp();
-            }
-            const bool keep = valid && !del;
-            const uint32_t km = __ballot_sync(kFull, keep);
-            const uint32_t pos = w + __popc(km & lanemask_lt());
-            __syncwarp();
-            if (keep && pos != k) write_slot(view, d.off + pos, x);
-            w += __popc(km);
-        }
+        const uint32_t w = (ge - gs <= 32u) ? warp_delete_regs(view, d, keys, gs, ge - gs, stage)
+                                            : warp_delete_global(view, d, u, keys, gs, ge, matched);
         if (lane == 0) {
             desc[u].deg = w;
             removed += d.deg - w;
@@ -209,9 +311,17 @@ __global__ void mutate_delete(AdjView view, RowDesc *desc, const unsigned long l
 }
 
 // Deletion phase for rows above kWarpRowMax: one block per row, tiles of
-// kTpbMut entries, candidates resolved in position order by one thread,
-// block scan for the in-place compaction.
+// kTpbMut x 8 entries (each thread two 16-byte loads), the group's keys and
+// matched counts in shared memory (up to kBigKeys keys; beyond that the
+// sorted keys and `matched` stay in global memory), a 4096-bit filter in
+// front of the key search, candidates resolved in position order by one
+// thread, and a block scan for the in-place compaction.
 constexpr int kTpbMut = 256;
+constexpr int kBigItems = 8;
+constexpr uint32_t kBigKeys = 2048;
+constexpr uint32_t kFilterBits = 4096;
+
+__device__ __forceinline__ uint32_t filter_hash(uint32_t x) { return (x * 0x9E3779B1u) >> 20; }  // 12 bits
 
 __global__ void __launch_bounds__(kTpbMut) mutate_delete_big(AdjView view, RowDesc *desc,
                                                               const unsigned long long *keys, uint32_t m,
@@ -220,54 +330,132 @@ __global__ void __launch_bounds__(kTpbMut) mutate_delete_big(AdjView view, RowDe
                                                               Status *st) {
     using BlockScan = cub::BlockScan<uint32_t, kTpbMut>;
     __shared__ typename BlockScan::TempStorage scan_tmp;
-    __shared__ uint32_t cand_bits[kTpbMut / 32];
-    __shared__ uint32_t del_bits[kTpbMut / 32];
-    __shared__ uint32_t cand_run[kTpbMut];
-    __shared__ uint32_t cand_req[kTpbMut];
+    __shared__ uint32_t skey[kBigKeys];
+    __shared__ uint32_t scount[kBigKeys];
+    __shared__ uint32_t filter[kFilterBits / 32];
+    __shared__ uint8_t cand_bits[kTpbMut];
+    __shared__ uint8_t del_bits[kTpbMut];
+    __shared__ uint16_t cand_run[kTpbMut * kBigItems];
+    __shared__ uint32_t g_run[kTpbMut * kBigItems];
+    __shared__ uint32_t stage[kTpbMut * kBigItems];
+    __shared__ uint32_t any_cand;
     const uint32_t tid = threadIdx.x;
     const uint32_t nb = *big_count;
     for (uint32_t g = blockIdx.x; g < nb; g += gridDim.x) {
         const uint32_t gs = big[g];
         const uint32_t ge = group_end(keys, m, gs);
+        const uint32_t gm = ge - gs;
+        const bool in_smem = gm <= kBigKeys;
         const uint32_t u = key_src(keys[gs]);
         const RowDesc d = desc[u];
         const unsigned long long uhi = static_cast<unsigned long long>(u) << kKeyShift;
-        uint32_t w = 0;
-        for (uint32_t base = 0; base < d.deg; base += kTpbMut) {
-            const uint32_t k = base + tid;
-            const bool valid = k < d.deg;
-            const uint32_t x = valid ? *view.at(d.off + k) : 0u;
-            uint32_t run = 0, req = 0;
-            const bool cand = valid && find_run(keys, gs, ge, uhi | x, run, req);
-            cand_run[tid] = run;
-            cand_req[tid] = req;
-            const uint32_t bits = __ballot_sync(kFull, cand);
-            if ((tid & 31u) == 0) {
-                cand_bits[tid >> 5] = bits;
-                del_bits[tid >> 5] = 0;
+        for (uint32_t i = tid; i < kFilterBits / 32; i += kTpbMut) filter[i] = 0;
+        __syncthreads();
+        for (uint32_t j = tid; j < gm; j += kTpbMut) {
+            const uint32_t x = key_low(keys[gs + j]);
+            if (in_smem) {
+                skey[j] = x;
+                scount[j] = 0;
             }
-            __syncthreads();
-            if (tid == 0) {
-                for (uint32_t wi = 0; wi < kTpbMut / 32; ++wi) {
-                    uint32_t b = cand_bits[wi];
-                    while (b) {
-                        const uint32_t bit = __ffs(b) - 1;
-                        b &= b - 1;
-                        const uint32_t p = wi * 32 + bit;
-                        const uint32_t r = cand_run[p];
-                        const uint32_t seen = matched[r];
-                        if (seen < cand_req[p]) del_bits[wi] |= 1u << bit;
-                        matched[r] = seen + 1;
+            const uint32_t h = filter_hash(x);
+            atomicOr(&filter[h >> 5], 1u << (h & 31u));
+        }
+        __syncthreads();
+        uint32_t w = 0;
+        for (uint32_t base = 0; base < d.deg; base += kTpbMut * kBigItems) {
+            const uint32_t k0 = base + tid * kBigItems;
+            uint32_t e[kBigItems];
+#pragma unroll
+            for (int h = 0; h < kBigItems; h += 4) {
+                if (k0 + h < d.deg) {
+                    const uint4 q = *reinterpret_cast<const uint4 *>(view.at(d.off + k0 + h));
+                    e[h] = q.x;
+                    e[h + 1] = q.y;
+                    e[h + 2] = q.z;
+                    e[h + 3] = q.w;
+                } else {
+                    e[h] = e[h + 1] = e[h + 2] = e[h + 3] = 0;
+                }
+            }
+            uint32_t cb = 0;
+#pragma unroll
+            for (int s = 0; s < kBigItems; ++s) {
+                if (k0 + s >= d.deg) continue;
+                const uint32_t h = filter_hash(e[s]);
+                if (!((filter[h >> 5] >> (h & 31u)) & 1u)) continue;
+                if (in_smem) {
+                    uint32_t lo = 0, hi = gm;
+                    while (lo < hi) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (skey[mid] < e[s])
+                            lo = mid + 1;
+                        else
+                            hi = mid;
+                    }
+                    if (lo < gm && skey[lo] == e[s]) {
+                        cb |= 1u << s;
+                        cand_run[tid * kBigItems + s] = static_cast<uint16_t>(lo);
+                    }
+                } else {
+                    uint32_t run, req;
+                    if (find_run(keys, gs, ge, uhi | e[s], run, req)) {
+                        cb |= 1u << s;
+                        g_run[tid * kBigItems + s] = run;
                     }
                 }
             }
+            cand_bits[tid] = static_cast<uint8_t>(cb);
+            del_bits[tid] = 0;
+            if (tid == 0) any_cand = 0;
             __syncthreads();
-            const bool del = (del_bits[tid >> 5] >> (tid & 31u)) & 1u;
-            const uint32_t keep = (valid && !del) ? 1u : 0u;
+            if (cb) any_cand = 1;
+            __syncthreads();
+            if (any_cand) {
+                if (tid == 0) {
+                    for (uint32_t t = 0; t < kTpbMut; ++t) {
+                        uint32_t b = cand_bits[t];
+                        uint32_t dbits = 0;
+                        while (b) {
+                            const uint32_t s = __ffs(b) - 1;
+                            b &= b - 1;
+                            bool del;
+                            if (in_smem) {
+                                const uint32_t r = cand_run[t * kBigItems + s];
+                                uint32_t e2 = r + 1;
+                                while (e2 < gm && skey[e2] == skey[r]) ++e2;
+                                del = scount[r] < e2 - r;
+                                scount[r] += 1;
+                            } else {
+                                const uint32_t r = g_run[t * kBigItems + s];
+                                uint32_t e2 = r + 1;
+                                while (e2 < ge && keys[e2] == keys[r]) ++e2;
+                                del = matched[r] < e2 - r;
+                                matched[r] += 1;
+                            }
+                            if (del) dbits |= 1u << s;
+                        }
+                        del_bits[t] = static_cast<uint8_t>(dbits);
+                    }
+                }
+                __syncthreads();
+            }
+            const uint32_t db = del_bits[tid];
+            uint32_t kc = 0;
+#pragma unroll
+            for (int s = 0; s < kBigItems; ++s) kc += (k0 + s < d.deg && !((db >> s) & 1u)) ? 1u : 0u;
             uint32_t prefix, total;
-            BlockScan(scan_tmp).ExclusiveSum(keep, prefix, total);
+            BlockScan(scan_tmp).ExclusiveSum(kc, prefix, total);
             __syncthreads();
-            if (keep && w + prefix != k) write_slot(view, d.off + w + prefix, x);
+            const uint32_t tile_valid = min(static_cast<uint32_t>(kTpbMut * kBigItems), d.deg - base);
+            if (w != base || total != tile_valid) {
+                // Stage the survivors, then store them with coalesced writes.
+                uint32_t pos = prefix;
+#pragma unroll
+                for (int s = 0; s < kBigItems; ++s)
+                    if (k0 + s < d.deg && !((db >> s) & 1u)) stage[pos++] = e[s];
+                __syncthreads();
+                for (uint32_t i = tid; i < total; i += kTpbMut) write_slot(view, d.off + w + i, stage[i]);
+            }
             w += total;
             __syncthreads();
         }

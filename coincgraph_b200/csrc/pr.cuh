@@ -76,7 +76,7 @@ struct PrPushOp {
     uint32_t cap;
     Status *st;
 
-    __device__ __forceinline__ void edge(bool valid, uint32_t, uint32_t item, uint32_t y) const {
+    __device__ __forceinline__ bool edge(bool valid, uint32_t, uint32_t item, uint32_t y) const {
         bool want = false;
         if (valid) {
             const T c = contrib[item];
@@ -87,6 +87,7 @@ struct PrPushOp {
                 want = atomicCAS(queued + y, 0u, 1u) == 0u;
         }
         warp_enqueue(want, y, q_out, q_cnt, cap, st);
+        return valid;
     }
 };
 
@@ -152,9 +153,7 @@ __global__ void __launch_bounds__(kTpbPr) pr_converge(AdjView fwd, PrArrays<T> a
         }
         if (!grid_barrier(st)) break;
     }
-    warp_count(&st->counters[kCntEdges], cnt.edges);
-    warp_count(&st->counters[kCntEdgesCached], cnt.edges_cached);
-    warp_count(&st->counters[kCntExpanded], cnt.rows);
+    flush_counters(st, cnt, kCntPr);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *a.final_round = r;
         atomicAdd(&st->counters[kCntPrRounds], static_cast<unsigned long long>(r));
@@ -233,9 +232,7 @@ __global__ void __launch_bounds__(kTpbPr) pr_amend_scatter(AdjView fwd, PrArrays
         }
         expand_rows<kTpbPr>(fwd, has, s, i, off, deg, op, sm, cnt);
     }
-    warp_count(&st->counters[kCntEdges], cnt.edges);
-    warp_count(&st->counters[kCntEdgesCached], cnt.edges_cached);
-    warp_count(&st->counters[kCntExpanded], cnt.rows);
+    flush_counters(st, cnt, kCntPr);
 }
 
 // FP64 L1 norm of the residual.

@@ -53,17 +53,19 @@ struct PushOp {
     uint32_t q_cap;
     Status *st;
 
-    __device__ __forceinline__ void edge(bool valid, uint32_t x, uint32_t dx, uint32_t y) const {
-        bool want = false;
+    __device__ __forceinline__ bool edge(bool valid, uint32_t x, uint32_t dx, uint32_t y) const {
+        bool want = false, improved = false;
         if (valid) {
             const uint32_t nd = dx + edge_weight<A>(x, y);
             const unsigned long long cand = pack(nd, x);
             if (cand < __ldcg(state + y)) {
                 const unsigned long long old = atomicMin(state + y, cand);
-                if (nd < val_of(old) && __ldcg(qstamp + y) != tag) want = atomicExch(qstamp + y, tag) != tag;
+                improved = nd < val_of(old);
+                if (improved && __ldcg(qstamp + y) != tag) want = atomicExch(qstamp + y, tag) != tag;
             }
         }
         warp_enqueue(want, y, q_out, q_count, q_cap, st);
+        return improved;
     }
 };
 
@@ -82,7 +84,7 @@ struct InvalOp {
     uint32_t cap;
     Status *st;
 
-    __device__ __forceinline__ void edge(bool valid, uint32_t x, uint32_t px, uint32_t z) const {
+    __device__ __forceinline__ bool edge(bool valid, uint32_t x, uint32_t px, uint32_t z) const {
         bool want = false;
         if (valid) {
             const unsigned long long sz = __ldcg(state + z);
@@ -94,6 +96,7 @@ struct InvalOp {
             if (dep && __ldcg(aff_stamp + z) != epoch) want = atomicExch(aff_stamp + z, epoch) != epoch;
         }
         warp_enqueue(want, z, list, count, cap, st);
+        return want;
     }
 };
 
@@ -107,18 +110,20 @@ struct PullOp {
     const uint32_t *aff_stamp;
     uint32_t epoch;
 
-    __device__ __forceinline__ void edge(bool valid, uint32_t v, uint32_t, uint32_t u) const {
-        if (!valid) return;
+    __device__ __forceinline__ bool edge(bool valid, uint32_t v, uint32_t, uint32_t u) const {
+        if (!valid) return false;
         unsigned long long cand;
         if (__ldcg(aff_stamp + u) == epoch) {
-            if (A != kCc) return;
+            if (A != kCc) return false;
             cand = pack(u, u);
         } else {
             const uint32_t du = val_of(__ldcg(state + u));
-            if (du == kInf) return;
+            if (du == kInf) return false;
             cand = pack(du + edge_weight<A>(u, v), u);
         }
-        if (cand < __ldcg(state + v)) atomicMin(state + v, cand);
+        if (cand >= __ldcg(state + v)) return false;
+        atomicMin(state + v, cand);
+        return true;
     }
 };
 
@@ -164,10 +169,7 @@ __global__ void __launch_bounds__(kTpb) push_closure(AdjView fwd, unsigned long 
         }
         if (!grid_barrier(st)) break;
     }
-    // Counters (one atomic per warp).
-    warp_count(&st->counters[kCntEdges], cnt.edges);
-    warp_count(&st->counters[kCntEdgesCached], cnt.edges_cached);
-    warp_count(&st->counters[kCntExpanded], cnt.rows);
+    flush_counters(st, cnt, kCntPush);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         atomicAdd(&st->counters[kCntRounds], static_cast<unsigned long long>(r));
         tags->next_tag = tag0 + r + 1;
@@ -214,9 +216,7 @@ __global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long
         lo = hi;
         hi = hi + ld_volatile(cnt3 + ((r + 1) % 3));
     }
-    warp_count(&st->counters[kCntEdges], c.edges);
-    warp_count(&st->counters[kCntEdgesCached], c.edges_cached);
-    warp_count(&st->counters[kCntExpanded], c.rows);
+    flush_counters(st, c, kCntInval);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *aff_total = hi;
         atomicAdd(&st->counters[kCntRounds], static_cast<unsigned long long>(r));
@@ -284,9 +284,7 @@ __global__ void __launch_bounds__(kTpb) pull_repair(AdjView rev, unsigned long l
         }
         expand_rows<kTpb>(rev, has, v, 0u, off, deg, op, sm, c);
     }
-    warp_count(&st->counters[kCntEdges], c.edges);
-    warp_count(&st->counters[kCntEdgesCached], c.edges_cached);
-    warp_count(&st->counters[kCntExpanded], c.rows);
+    flush_counters(st, c, kCntPull);
 }
 
 // Queue every repaired vertex that has a value (all of them for CC).

@@ -63,6 +63,7 @@ class BatchStats(ctypes.Structure):
         ("ms_cache", ctypes.c_double),
         ("pr_rounds", ctypes.c_uint64),
         ("pr_residual_l1", ctypes.c_double),
+        ("kernel_launches", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:
@@ -81,6 +82,23 @@ class GraphInfo(ctypes.Structure):
         ("cache_capacity_segments", ctypes.c_uint64),
         ("device_bytes", ctypes.c_uint64),
         ("pinned_bytes", ctypes.c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+STAGES = ["group", "mutate", "seed", "inval", "pull", "push", "pr", "cache", "mutate_rev"]
+
+
+class StageProfile(ctypes.Structure):
+    _fields_ = [
+        ("ms", ctypes.c_double),
+        ("launches", ctypes.c_uint64),
+        ("edges", ctypes.c_uint64),
+        ("edges_cached", ctypes.c_uint64),
+        ("rows", ctypes.c_uint64),
+        ("hits", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:
@@ -112,6 +130,8 @@ SIGNATURES = [
     ("cig_get_row", _i32, [_vp, _u32, _vp, _u32, ctypes.POINTER(_u32)]),
     ("cig_export_csr", _i32, [_vp, _vp, _vp]),
     ("cig_graph_info_get", _i32, [_vp, ctypes.POINTER(GraphInfo)]),
+    ("cig_profile_enable", _i32, [_vp, _i32]),
+    ("cig_profile_read", _i32, [_vp, ctypes.POINTER(StageProfile), _u32]),
     ("cig_query_bfs_multi", _i32, [_vp, _vp, _u32, _vp]),
     ("cig_query_sssp_multi", _i32, [_vp, _vp, _u32, _vp]),
     ("cig_version", ctypes.c_char_p, []),
@@ -304,6 +324,15 @@ class Engine:
         adj = np.empty(max(int(xadj[-1]), 1), dtype=np.uint32)
         self._check(self.lib.cig_export_csr(self.h, _ptr(xadj), _ptr(adj)))
         return xadj, adj[: int(xadj[-1])]
+
+    def profile(self, enable: bool = True):
+        """Clear the per-stage accumulators and turn stage timing on/off."""
+        self._check(self.lib.cig_profile_enable(self.h, int(enable)))
+
+    def profile_read(self) -> dict:
+        arr = (StageProfile * len(STAGES))()
+        self._check(self.lib.cig_profile_read(self.h, arr, len(STAGES)))
+        return {name: arr[i].as_dict() for i, name in enumerate(STAGES)}
 
     def info(self) -> dict:
         g = GraphInfo()

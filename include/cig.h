@@ -81,6 +81,7 @@ typedef struct {
     double ms_cache;             /* device time of cache maintenance */
     uint64_t pr_rounds;
     double pr_residual_l1;       /* FP64 L1 norm of the PR residual after the batch */
+    uint64_t kernel_launches;    /* engine kernels launched by the call (library sort kernels excluded) */
 } cig_batch_stats;
 
 typedef struct {
@@ -168,6 +169,36 @@ int cig_graph_info_get(cig_handle *h, cig_graph_info *info);
  * frontiers.  Does not change the maintained state. */
 int cig_query_bfs_multi(cig_handle *h, const uint32_t *sources, uint32_t k, uint32_t *out_depth);
 int cig_query_sssp_multi(cig_handle *h, const uint32_t *sources, uint32_t k, uint32_t *out_dist);
+
+/* Per-stage device time and work counters, measured with CUDA events on the
+ * engine's own stream.  Replaces the reference's [ATTR] stage attribution
+ * (samples/hybrid_sssp/hybrid_sssp.cu:496-512) and its NVTX marks
+ * (include/utils/markers.h).  cig_profile_enable(h, 1) clears and starts the
+ * accumulators; cig_profile_read copies CIG_STAGE_COUNT entries. */
+enum {
+    CIG_STAGE_GROUP = 0,  /* update keys, radix sort, source groups */
+    CIG_STAGE_MUTATE = 1, /* forward rows: deletion/append/relocation, block allocation */
+    CIG_STAGE_SEED = 2,   /* deletion and insertion seeds */
+    CIG_STAGE_INVAL = 3,  /* invalidation closure */
+    CIG_STAGE_PULL = 4,   /* reset + pull repair over in-rows + re-queue */
+    CIG_STAGE_PUSH = 5,   /* push closure */
+    CIG_STAGE_PR = 6,     /* PageRank amend + converge */
+    CIG_STAGE_CACHE = 7,  /* edge-cache maintenance */
+    CIG_STAGE_MUTATE_REV = 8, /* reverse (in-edge) rows */
+    CIG_STAGE_COUNT = 9
+};
+
+typedef struct {
+    double ms;              /* summed device time */
+    uint64_t launches;      /* timed regions */
+    uint64_t edges;         /* adjacency entries read (traversal stages) */
+    uint64_t edges_cached;  /* of which from HBM */
+    uint64_t rows;          /* rows expanded */
+    uint64_t hits;          /* relaxations / invalidations / residual pushes */
+} cig_stage_profile;
+
+int cig_profile_enable(cig_handle *h, int enable);
+int cig_profile_read(cig_handle *h, cig_stage_profile *out, uint32_t count);
 
 /* Library version string. */
 const char *cig_version(void);

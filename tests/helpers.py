@@ -107,6 +107,30 @@ def big_row_case() -> Case:
     return Case("bigrow", n, xadj, adj, batches, source=0)
 
 
+def heavy_delete_case() -> Case:
+    """Many deletion keys in one row: a 3000-entry row losing 200 entries
+    (more than a warp's 32 key registers) and a 12000-entry row losing 3000
+    (more than the block path's 2048 shared-memory keys), with parallel edges
+    and repeated requests."""
+    rng = np.random.default_rng(11)
+    n = 9000
+    src = np.concatenate([np.full(3000, 0), np.full(12000, 1), rng.integers(0, n, 20000)])
+    dst = np.concatenate([rng.integers(2, 400, 3000), rng.integers(2, n, 12000), rng.integers(0, n, 20000)])
+    xadj, adj = _csr_from_edges(n, src, dst)
+    row0 = adj[int(xadj[0]):int(xadj[1])]
+    row1 = adj[int(xadj[1]):int(xadj[2])]
+    batches = []
+    for k in range(2):
+        d0 = row0[rng.integers(0, len(row0), 200)]
+        d1 = row1[rng.integers(0, len(row1), 3000)]
+        du = np.concatenate([np.zeros(200, np.uint32), np.ones(3000, np.uint32)])
+        dv = np.concatenate([d0, d1]).astype(np.uint32)
+        au = rng.integers(0, n, 500).astype(np.uint32)
+        av = rng.integers(0, n, 500).astype(np.uint32)
+        batches.append((du, dv, au, av))
+    return Case("heavydelete", n, xadj, adj, batches, source=0)
+
+
 ORACLE_MODE = {"bfs": 0, "sssp": 1, "cc": 2}
 
 

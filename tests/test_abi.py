@@ -56,4 +56,5 @@ def test_struct_layouts(built):
     from coincgraph_b200 import engine
 
     assert ctypes.sizeof(engine.Options) == 48
-    assert ctypes.sizeof(engine.BatchStats) == 19 * 8
+    assert ctypes.sizeof(engine.BatchStats) == 20 * 8
+    assert ctypes.sizeof(engine.StageProfile) == 6 * 8

@@ -13,7 +13,7 @@ import pytest
 
 import oracle
 from coincgraph_b200 import Engine
-from helpers import ORACLE_MODE, adversarial_case, big_row_case, oracle_trace, rmat_case
+from helpers import ORACLE_MODE, adversarial_case, big_row_case, heavy_delete_case, oracle_trace, rmat_case
 
 pytestmark = pytest.mark.gpu
 
@@ -66,6 +66,12 @@ def test_adversarial(algo):
 @pytest.mark.parametrize("cache", ["resident", "mixed"])
 def test_big_rows(algo, cache):
     run_case(big_row_case(), algo, CACHES[cache])
+
+
+@pytest.mark.parametrize("algo", ["sssp", "cc"])
+@pytest.mark.parametrize("cache", ["resident", "zerocopy"])
+def test_heavy_deletions(algo, cache):
+    run_case(heavy_delete_case(), algo, CACHES[cache])
 
 
 @pytest.mark.parametrize("algo", ["bfs", "sssp", "cc"])

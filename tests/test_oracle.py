@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 import oracle
-from helpers import adversarial_case, big_row_case, rmat_case
+from helpers import adversarial_case, big_row_case, heavy_delete_case, rmat_case
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 needs_ref = pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built (no reference tree)")
@@ -23,7 +23,8 @@ def _rows_equal(a, b):
 
 
 @needs_ref
-@pytest.mark.parametrize("make", [adversarial_case, big_row_case, lambda: rmat_case(10, 5, 80, 80, seed_offset=3)])
+@pytest.mark.parametrize("make", [adversarial_case, big_row_case, heavy_delete_case,
+                                  lambda: rmat_case(10, 5, 80, 80, seed_offset=3)])
 def test_rows_match_reference_store(built, make):
     case = make()
     g = oracle.Graph(case.n, case.xadj, case.adj)
