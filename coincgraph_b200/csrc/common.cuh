@@ -36,12 +36,24 @@ enum : uint32_t {
     kErrInternal = 1u << 5,
 };
 
+// A deleted entry is overwritten with kTomb (never a vertex id: ids are
+// below n <= 2^32 - 1).  Survivors keep their relative order, so a row with
+// its tombstones removed is exactly the row the reference keeps; tombstones
+// are dropped when the row is compacted or relocated.
+constexpr uint32_t kTomb = 0xFFFFFFFFu;
+constexpr uint32_t kMaxTombs = (1u << 26) - 1;
+
 struct RowDesc {
-    uint64_t off;  // first slot of the block in the arena
-    uint32_t deg;  // live entries
-    uint32_t cls;  // block holds 2^cls slots; 0 = no block
+    uint64_t off;   // first slot of the block in the arena
+    uint32_t len;   // used slots (live entries + tombstones)
+    uint32_t meta;  // bits 0-5: class (block holds 2^cls slots, 0 = no block); bits 6-31: tombstones
 };
 static_assert(sizeof(RowDesc) == 16, "RowDesc must stay 16 bytes");
+
+__host__ __device__ __forceinline__ uint32_t rd_cls(const RowDesc &d) { return d.meta & 63u; }
+__host__ __device__ __forceinline__ uint32_t rd_tombs(const RowDesc &d) { return d.meta >> 6; }
+__host__ __device__ __forceinline__ uint32_t rd_live(const RowDesc &d) { return d.len - (d.meta >> 6); }
+__host__ __device__ __forceinline__ uint32_t rd_meta(uint32_t cls, uint32_t tombs) { return cls | (tombs << 6); }
 
 // Device view of one arena.  For the forward arena `seg_slot` maps segments
 // to cache slots (-1 = host); for a device-only arena it is null and `dev`

@@ -109,7 +109,7 @@ Layout plan_layout(uint32_t n, const uint32_t *deg) {
     for (uint32_t v = 0; v < n; ++v) {
         if (!deg[v]) continue;
         const uint32_t c = host_class(deg[v]);
-        L.desc[v] = RowDesc{cursor[c], deg[v], c};
+        L.desc[v] = RowDesc{cursor[c], deg[v], rd_meta(c, 0)};
         cursor[c] += 1ull << c;
     }
     return L;
@@ -173,8 +173,12 @@ enum SmallIdx : int {
     kBigR = 10,
     kTouched = 11,
     kFinalRound = 12,
-    kSmallCount = 16
+    kBigRows = 13,  // 3 counters of deferred hub rows
+    kCompactCount = 16,
+    kSmallCount = 20
 };
+
+constexpr uint32_t kBigRowCap = 65536;
 
 struct DevArena {
     RowDesc *desc = nullptr;
@@ -253,6 +257,7 @@ struct cig_handle {
     uint32_t *gf = nullptr, *gr = nullptr, *mf = nullptr, *mr = nullptr, *bigf = nullptr, *bigr = nullptr;
     unsigned long long *pf = nullptr, *prr = nullptr;
     uint32_t *touched = nullptr;
+    uint32_t *compact = nullptr;  // rows queued for tombstone compaction
     void *cub = nullptr;
     size_t cub_bytes = 0;
     uint32_t *stage = nullptr;  // pinned staging for host update arrays (4 * bcap)
@@ -322,6 +327,13 @@ struct cig_handle {
     int persistent_grid() const { return sms * 8; }
 
     Frontier frontier() const { return Frontier{q0, q1, small + kFr, n + 1}; }
+
+    BigRow *big_rows = nullptr;
+    // Deferred hub rows; the counters are cleared before every launch that uses them.
+    BigList big_list() {
+        CK(cudaMemsetAsync(small + kBigRows, 0, 3 * sizeof(uint32_t), stream));
+        return BigList{big_rows, small + kBigRows, kBigRowCap};
+    }
 
     template <class K>
     int coop_blocks(K kernel, int tpb) const {
@@ -418,6 +430,7 @@ struct cig_handle {
         dmalloc(small, kSmallCount);
         CK(cudaMemset(small, 0, kSmallCount * sizeof(uint32_t)));
         dmalloc(small64, 4);
+        dmalloc(big_rows, kBigRowCap);
         dmalloc(tags, 1);
         CK(cudaMemset(tags, 0, sizeof(TagState)));
         pr64 = (opt.flags & CIG_FLAG_PR_FP64) != 0;
@@ -448,6 +461,7 @@ struct cig_handle {
         dfree(list);
         dfree(small);
         dfree(small64);
+        dfree(big_rows);
         dfree(tags);
         dfree(status);
         if (h_status) cudaFreeHost(h_status);
@@ -480,6 +494,7 @@ struct cig_handle {
         dfree(pf);
         dfree(prr);
         dfree(touched);
+        dfree(compact);
         dfree(cub);
         if (stage) cudaFreeHost(stage);
         stage = nullptr;
@@ -509,6 +524,7 @@ struct cig_handle {
         dmalloc(pf, cap);
         dmalloc(prr, cap);
         dmalloc(touched, 2 * cap);
+        dmalloc(compact, cap);
         if (opt.algo == CIG_PR) {
             dfree(pr_amend);
             CK(cudaMalloc(&pr_amend, 2 * cap * (pr64 ? sizeof(double) : sizeof(float))));
@@ -718,7 +734,8 @@ struct cig_handle {
     template <int A>
     void run_push() {
         const int p = prof_begin(CIG_STAGE_PUSH);
-        launch_coop(push_closure<A>, kTpb, fwd.view(), state, qstamp, tags, frontier(), n + 2, seg_hot, status);
+        launch_coop(push_closure<A>, kTpb, fwd.view(), state, qstamp, tags, frontier(), big_list(), n + 2, seg_hot,
+                    status);
         prof_end(p);
     }
 
@@ -821,10 +838,13 @@ struct cig_handle {
         prof_end(p);
         p = prof_begin(forward ? CIG_STAGE_MUTATE : CIG_STAGE_MUTATE_REV);
         unsigned long long *stats = with_stats ? status->counters : nullptr;
-        launch(mutate_delete, persistent_grid(), 256, A.view(), A.desc, sorted, m, groups, gcount, matched,
-                                                             big, bcount, stats, status);
-        launch(mutate_delete_big, sms * 2, kTpbMut, A.view(), A.desc, sorted, m, big, bcount, matched,
-                                                           stats, status);
+        uint32_t *ccount = small + kCompactCount;
+        CK(cudaMemsetAsync(ccount, 0, sizeof(uint32_t), stream));
+        launch(mutate_delete, persistent_grid(), kMutWarps * 32, A.view(), A.desc, sorted, m, groups, gcount,
+               matched, big, bcount, compact, ccount, stats, status);
+        launch(mutate_delete_big, sms * 4, kTpbMut, A.view(), A.desc, sorted, m, big, bcount, matched, compact,
+               ccount, stats, status);
+        launch(compact_rows, sms * 4, kTpbMut, A.view(), A.desc, compact, ccount);
         prof_end(p);
         check_launch();
     }
@@ -877,13 +897,15 @@ struct cig_handle {
         mutate_delete_arena(fwd, d_du, d_dv, nd, true, true);
         mutate_delete_arena(rev, d_du, d_dv, nd, false, false);
         p = prof_begin(CIG_STAGE_INVAL);
-        launch_coop(inval_closure<A>, kTpb, fwd.view(), state, aff_stamp, epoch, list, small + kAff, n + 1, n + 2,
-                    small + kAffTotal, status);
+        launch_coop(inval_closure<A>, kTpb, fwd.view(), state, aff_stamp, epoch, list, small + kAff, n + 1,
+                    big_list(), n + 2, small + kAffTotal, status);
         prof_end(p);
         p = prof_begin(CIG_STAGE_PULL);
         launch(reset_affected<A>, persistent_grid(), 256, list, small + kAffTotal, state);
+        const BigList pull_big = big_list();
         launch(pull_repair<A>, persistent_grid(), kTpb, rev.view(), state, aff_stamp, epoch, list,
-                                                               small + kAffTotal, status);
+                                                               small + kAffTotal, pull_big, status);
+        launch(pull_deferred<A>, persistent_grid(), kTpb, rev.view(), state, aff_stamp, epoch, pull_big, status);
         launch(enqueue_affected<A>, persistent_grid(), 256, list, small + kAffTotal, state, frontier(), status);
         prof_end(p);
         check_launch();
@@ -1249,7 +1271,7 @@ int cig_num_edges(cig_handle *h, uint64_t *m) {
         if (!m) throw CigError(CIG_ERR_ARG, "null output");
         const auto d = h->host_desc();
         uint64_t s = 0;
-        for (const auto &r : d) s += r.deg;
+        for (const auto &r : d) s += rd_live(r);
         *m = s;
     });
 }
@@ -1258,8 +1280,19 @@ int cig_get_degrees(cig_handle *h, uint32_t *deg) {
     return guarded(h, [&] {
         if (!deg) throw CigError(CIG_ERR_ARG, "null output");
         const auto d = h->host_desc();
-        for (uint32_t v = 0; v < h->n; ++v) deg[v] = d[v].deg;
+        for (uint32_t v = 0; v < h->n; ++v) deg[v] = rd_live(d[v]);
     });
+}
+
+// Copy the live entries of a row (tombstones dropped, order kept).
+static uint32_t copy_live(const uint32_t *row, uint32_t len, uint32_t *out, uint32_t capacity) {
+    uint32_t w = 0;
+    for (uint32_t k = 0; k < len; ++k) {
+        if (row[k] == kTomb) continue;
+        if (out && w < capacity) out[w] = row[k];
+        ++w;
+    }
+    return w;
 }
 
 int cig_get_row(cig_handle *h, uint32_t v, uint32_t *out, uint32_t capacity, uint32_t *degree) {
@@ -1269,8 +1302,8 @@ int cig_get_row(cig_handle *h, uint32_t v, uint32_t *out, uint32_t capacity, uin
         RowDesc d;
         h->flush_host();
         CK(cudaMemcpy(&d, h->fwd.desc + v, sizeof(d), cudaMemcpyDeviceToHost));
-        if (degree) *degree = d.deg;
-        if (out) std::memcpy(out, h->fwd.host + d.off, std::min(capacity, d.deg) * sizeof(uint32_t));
+        if (degree) *degree = rd_live(d);
+        if (out) copy_live(h->fwd.host + d.off, d.len, out, capacity);
     });
 }
 
@@ -1279,13 +1312,13 @@ int cig_export_csr(cig_handle *h, uint64_t *xadj, uint32_t *adj) {
         if (!xadj) throw CigError(CIG_ERR_ARG, "null output");
         const auto d = h->host_desc();
         xadj[0] = 0;
-        for (uint32_t v = 0; v < h->n; ++v) xadj[v + 1] = xadj[v] + d[v].deg;
+        for (uint32_t v = 0; v < h->n; ++v) xadj[v + 1] = xadj[v] + rd_live(d[v]);
         if (!adj) return;
         h->flush_host();
         const uint32_t *arena = h->fwd.host;
         parallel_for(h->n, [&](uint64_t b, uint64_t e) {
             for (uint64_t v = b; v < e; ++v)
-                if (d[v].deg) std::memcpy(adj + xadj[v], arena + d[v].off, d[v].deg * sizeof(uint32_t));
+                if (d[v].len) copy_live(arena + d[v].off, d[v].len, adj + xadj[v], rd_live(d[v]));
         });
     });
 }
@@ -1298,7 +1331,7 @@ int cig_graph_info_get(cig_handle *h, cig_graph_info *info) {
         if (!h->loaded) return;
         const auto d = h->host_desc();
         uint64_t m = 0;
-        for (const auto &r : d) m += r.deg;
+        for (const auto &r : d) m += rd_live(r);
         info->m = m;
         ArenaAlloc al;
         CK(cudaMemcpy(&al, h->fwd.alloc, sizeof(al), cudaMemcpyDeviceToHost));

@@ -49,19 +49,44 @@ __device__ __forceinline__ void flush_counters(Status *st, const ExpandCounters 
     warp_count(&st->counters[group + 3], c.hits);
 }
 
+// Rows with at least kSplitDeg entries are not expanded by the block that
+// holds them: they are appended to a list that every block of the grid
+// then expands in kSplitChunk-entry chunks (expand_deferred), so that one
+// hub row does not serialise a whole round on one block.
+constexpr uint32_t kSplitDeg = 4096;
+constexpr uint32_t kSplitChunk = 1024;
+
+struct BigRow {
+    unsigned long long off;
+    uint32_t x, payload, deg, pad;
+};
+
+struct Defer {
+    BigRow *rows;     // null: expand every row in place
+    uint32_t *count;
+    uint32_t cap;
+};
+
 // Op must provide: __device__ bool edge(bool valid, uint32_t x, uint32_t payload, uint32_t y) const;
 // returning true when the edge changed state.
 // edge() is called by all 32 lanes of a warp together (valid=false on padding lanes).
 template <int TPB, class Op>
 __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint32_t x, uint32_t payload,
                                             uint64_t off, uint32_t deg, const Op &op, ExpandSmem<TPB> &sm,
-                                            ExpandCounters &cnt) {
+                                            ExpandCounters &cnt, const Defer &defer = Defer{nullptr, nullptr, 0}) {
     const uint32_t lane = lane_id();
     const uint32_t warp = threadIdx.x >> 5;
     if (has) {
         cnt.rows += 1;
         cnt.edges += deg;
         if (view.cached(off)) cnt.edges_cached += deg;
+    }
+    if (has && defer.rows && deg >= kSplitDeg) {
+        const uint32_t i = atomicAdd(defer.count, 1u);
+        if (i < defer.cap) {
+            defer.rows[i] = BigRow{off, x, payload, deg, 0u};
+            has = false;
+        }
     }
 
     // Tier 1: block-wide rows.  Rows larger than one segment are resolved
@@ -86,14 +111,14 @@ __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint3
                 const uint32_t k = base + threadIdx.x;
                 const bool valid = k < bdeg;
                 const uint32_t y = valid ? __ldg(rp + k) : 0u;
-                cnt.hits += op.edge(valid, bx, bp, y);
+                cnt.hits += op.edge(valid && y != kTomb, bx, bp, y);
             }
         } else {
             for (uint32_t base = 0; base < bdeg; base += TPB) {
                 const uint32_t k = base + threadIdx.x;
                 const bool valid = k < bdeg;
                 const uint32_t y = valid ? __ldg(view.at(boff + k)) : 0u;
-                cnt.hits += op.edge(valid, bx, bp, y);
+                cnt.hits += op.edge(valid && y != kTomb, bx, bp, y);
             }
         }
         __syncthreads();
@@ -114,7 +139,7 @@ __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint3
             const uint32_t k = base + lane;
             const bool valid = k < wdeg;
             const uint32_t y = valid ? __ldg(rp + k) : 0u;
-            cnt.hits += op.edge(valid, wx, wp, y);
+            cnt.hits += op.edge(valid && y != kTomb, wx, wp, y);
         }
     }
 
@@ -152,9 +177,34 @@ __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint3
             op_ = sm.f_payload[wb + lo];
             y = __ldg(sm.f_ptr[wb + lo] + (e - sm.f_scan[wb + lo]));
         }
-        cnt.hits += op.edge(valid, ox, op_, y);
+        cnt.hits += op.edge(valid && y != kTomb, ox, op_, y);
     }
     __syncwarp();
+}
+
+// Expand the deferred rows: chunk g of the concatenated chunk sequence goes
+// to block g mod gridDim.x.  Every block walks the (short) list in the same
+// order, so the assignment needs no coordination.  Block-uniform loops.
+template <int TPB, class Op>
+__device__ __forceinline__ void expand_deferred(const AdjView &view, const BigRow *rows, uint32_t nrows,
+                                                const Op &op, ExpandCounters &cnt) {
+    const uint32_t grid = gridDim.x;
+    uint64_t prefix = 0;
+    for (uint32_t i = 0; i < nrows; ++i) {
+        const BigRow r = rows[i];
+        const uint64_t chunks = (r.deg + kSplitChunk - 1) / kSplitChunk;
+        uint64_t g = prefix + (blockIdx.x + grid - static_cast<uint32_t>(prefix % grid)) % grid;
+        for (; g < prefix + chunks; g += grid) {
+            const uint32_t base = static_cast<uint32_t>(g - prefix) * kSplitChunk;
+            for (uint32_t kk = 0; kk < kSplitChunk; kk += TPB) {
+                const uint32_t k = base + kk + threadIdx.x;
+                const bool valid = k < r.deg;
+                const uint32_t y = valid ? __ldg(view.at(r.off + k)) : 0u;
+                cnt.hits += op.edge(valid && y != kTomb, r.x, r.payload, y);
+            }
+        }
+        prefix += chunks;
+    }
 }
 
 }  // namespace cig

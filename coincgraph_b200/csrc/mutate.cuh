@@ -7,16 +7,21 @@
 //     its first min(k, present) occurrences; survivors keep their order
 //     (BuildDeletionPlan / ShouldDelete / CompactSourceInPlace);
 //   addition phase: destinations are appended in input order; a row that
-//     outgrows its power-of-two block moves to a block of the next class
+//     outgrows its power-of-two block moves to a larger block
 //     (RewriteSourceToNewBlock).
 // The batch is grouped by source with a device radix sort of 64-bit keys
 // (source << 32 | destination) for deletions and (source << 32 | input index)
 // for additions; the latter keeps input order inside a source, as the
 // reference's stable radix sort does (effective_update_batch.h:48-73).
 //
-// Design differences: the grouping, deletion matching, compaction,
-// allocation and appends all run on the GPU; the forward arena is written
-// through to both the pinned host copy and the HBM cache copy of the segment.
+// Design differences from the reference (same rows):
+//   - a deleted entry is overwritten with a tombstone instead of shifting
+//     the rest of the row; the scan of a row stops once every requested
+//     deletion of that row has been found, so a batch reads about half of
+//     each touched row and writes one word per deletion;
+//   - a row is compacted (tombstones dropped, order kept) when it relocates
+//     or when tombstones reach a quarter of its length;
+//   - grouping, matching, allocation and appends all run on the GPU.
 #pragma once
 
 #include <cub/block/block_scan.cuh>
@@ -28,13 +33,15 @@ namespace cig {
 constexpr uint32_t kKeyShift = 32;
 constexpr unsigned long long kKeyNone = ~0ull;
 constexpr uint32_t kWarpRowMax = 4096;  // larger rows use the block path
+constexpr int kMutWarps = 8;            // warps per block of the warp-path kernels
+constexpr int kTpbMut = 256;            // threads per block of the block-path kernels
 
 __device__ __forceinline__ uint32_t key_src(unsigned long long k) { return static_cast<uint32_t>(k >> kKeyShift); }
 __device__ __forceinline__ uint32_t key_low(unsigned long long k) { return static_cast<uint32_t>(k); }
 
 // Device-side block allocator: per class a partially used segment
 // [cur_next, cur_end) and a global bump pointer over whole segments.
-// Retired blocks are not reused (see ArenaAlloc users).
+// Blocks left by relocation are not reused.
 struct ArenaAlloc {
     unsigned long long seg_bump;
     unsigned long long seg_total;
@@ -125,8 +132,8 @@ __device__ __forceinline__ uint32_t group_end(const unsigned long long *keys, ui
     return lo;
 }
 
-// Deletion run of destination x inside the group [gs, ge): returns the index
-// of the run's first key (a unique run id) and its requested count.
+// Deletion run of key `key` inside the group [gs, ge): the index of the
+// run's first key (a unique run id) and its requested count.
 __device__ __forceinline__ bool find_run(const unsigned long long *keys, uint32_t gs, uint32_t ge,
                                          unsigned long long key, uint32_t &run, uint32_t &req) {
     uint32_t lo = gs, hi = ge;
@@ -149,73 +156,53 @@ __device__ __forceinline__ void write_slot(const AdjView &view, unsigned long lo
     *view.wptr(off) = value;
 }
 
-// Compact one 128-entry chunk of a row in place, given per-element keep
-// flags for the 4 consecutive elements each lane holds (positions
-// base + 4*lane + s).  The survivors are staged in shared memory and written
-// back with coalesced stores; nothing is written while no entry at or before
-// this chunk was deleted.  All 32 lanes call.
-__device__ __forceinline__ uint32_t warp_compact4(uint32_t *dst, uint32_t *stage, uint32_t w, uint32_t base,
-                                                  const uint32_t (&e)[4], const bool (&keep)[4], uint32_t valid) {
-    const uint32_t lane = lane_id();
-    const uint32_t kc = keep[0] + keep[1] + keep[2] + keep[3];
-    uint32_t incl = kc;
-#pragma unroll
-    for (uint32_t o = 1; o < 32u; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(kFull, incl, o);
-        if (lane >= o) incl += t;
-    }
-    const uint32_t total = __shfl_sync(kFull, incl, 31);
-    if (w == base && total == valid) return w + total;  // nothing moved yet
-    uint32_t pos = incl - kc;
-#pragma unroll
-    for (int s = 0; s < 4; ++s)
-        if (keep[s]) stage[pos++] = e[s];
-    __syncwarp();
-    for (uint32_t i = lane; i < total; i += 32u) dst[w + i] = stage[i];
-    __syncwarp();
-    return w + total;
+// Record the tombstones a row received; queue it for compaction when they
+// reach a quarter of its length.
+__device__ __forceinline__ void finish_row(RowDesc *desc, uint32_t u, const RowDesc &d, uint32_t removed,
+                                           uint32_t *compact, uint32_t *compact_count) {
+    if (!removed) return;
+    const uint32_t tombs = rd_tombs(d) + removed;
+    desc[u].meta = rd_meta(rd_cls(d), tombs);
+    if (4ull * tombs >= d.len || tombs >= kMaxTombs / 2) compact[atomicAdd(compact_count, 1u)] = u;
 }
 
-// Deletion of a group with at most 32 runs' keys: the destinations live in
-// lane registers (lane j holds key j), matched counts in the run-head lanes.
-// The row lies inside one segment (deg <= kWarpRowMax).
-__device__ __forceinline__ uint32_t warp_delete_regs(const AdjView &view, const RowDesc &d,
-                                                     const unsigned long long *keys, uint32_t gs, uint32_t m,
-                                                     uint32_t *stage) {
+// ---------------------------------------------------------------- deletion
+
+// Rows of at most kWarpRowMax slots, at most 32 keys: lane j holds key j;
+// run multiplicities and matched counts live in the run-head lanes.
+// Returns the number of tombstones written.
+__device__ __forceinline__ uint32_t warp_tomb_regs(const AdjView &view, const RowDesc &d,
+                                                   const unsigned long long *keys, uint32_t gs, uint32_t m) {
     const uint32_t lane = lane_id();
     const bool kvalid = lane < m;
     const uint32_t kd = kvalid ? key_low(keys[gs + lane]) : 0u;
     const uint32_t vmask = __ballot_sync(kFull, kvalid);
-    uint32_t peers = __match_any_sync(kFull, kd) & vmask;
-    const uint32_t req_here = kvalid ? __popc(peers) : 0u;  // multiplicity of this lane's run
-    uint32_t mcount = 0;                                     // matched so far (run-head lanes)
+    const uint32_t peers = __match_any_sync(kFull, kd) & vmask;
+    const uint32_t req_here = kvalid ? __popc(peers) : 0u;
+    uint32_t mcount = 0;
+    uint32_t left = m;  // requests not yet satisfied (uniform)
     const uint32_t *src = view.at(d.off);
-    uint32_t *dst = nullptr;  // resolved (and the segment marked dirty) on the first move
-    uint32_t w = 0;
-    for (uint32_t base = 0; base < d.deg; base += 128u) {
+    uint32_t *dst = nullptr;
+    uint4 q = make_uint4(0, 0, 0, 0);
+    if (4u * lane < d.len) q = *reinterpret_cast<const uint4 *>(src + 4u * lane);
+    for (uint32_t base = 0; base < d.len && left; base += 128u) {
         const uint32_t k0 = base + 4u * lane;
-        uint32_t e[4] = {0, 0, 0, 0};
-        if (k0 < d.deg) {
-            const uint4 q = *reinterpret_cast<const uint4 *>(src + k0);
-            e[0] = q.x;
-            e[1] = q.y;
-            e[2] = q.z;
-            e[3] = q.w;
-        }
+        const uint32_t e[4] = {q.x, q.y, q.z, q.w};
+        // prefetch the next chunk while this one is matched
+        if (base + 128u + 4u * lane < d.len) q = *reinterpret_cast<const uint4 *>(src + base + 128u + 4u * lane);
         int run[4] = {-1, -1, -1, -1};
         for (uint32_t j = 0; j < m; ++j) {
             const uint32_t kj = __shfl_sync(kFull, kd, j);
 #pragma unroll
             for (int s = 0; s < 4; ++s)
-                if (run[s] < 0 && k0 + s < d.deg && e[s] == kj) run[s] = static_cast<int>(j);
+                if (run[s] < 0 && k0 + s < d.len && e[s] == kj) run[s] = static_cast<int>(j);
         }
-        bool del[4] = {false, false, false, false};
         uint32_t cm[4];
 #pragma unroll
         for (int s = 0; s < 4; ++s) cm[s] = __ballot_sync(kFull, run[s] >= 0);
         uint32_t any = cm[0] | cm[1] | cm[2] | cm[3];
-        // Resolve candidates in position order (lane-major, then s).
-        while (any) {
+        bool del[4] = {false, false, false, false};
+        while (any) {  // position order: lane-major, then s
             const uint32_t l = __ffs(any) - 1;
             any &= any - 1;
 #pragma unroll
@@ -225,34 +212,38 @@ __device__ __forceinline__ uint32_t warp_delete_regs(const AdjView &view, const 
                     const uint32_t req = __shfl_sync(kFull, req_here, r);
                     const uint32_t seen = __shfl_sync(kFull, mcount, r);
                     if (lane == r) mcount = seen + 1;
-                    if (lane == l) del[s] = seen < req;
+                    if (seen < req) {
+                        --left;
+                        if (lane == l) del[s] = true;
+                    }
                 }
             }
         }
-        bool keep[4];
+        if (del[0] | del[1] | del[2] | del[3]) {
+            if (!dst) dst = view.wptr(d.off);
 #pragma unroll
-        for (int s = 0; s < 4; ++s) keep[s] = (k0 + s < d.deg) && !del[s];
-        const uint32_t valid = min(128u, d.deg - base);
-        if (!dst && (cm[0] | cm[1] | cm[2] | cm[3] | (w != base))) dst = view.wptr(d.off);
-        w = warp_compact4(dst, stage, w, base, e, keep, valid);
+            for (int s = 0; s < 4; ++s)
+                if (del[s]) dst[k0 + s] = kTomb;
+        }
+        __syncwarp();
     }
-    return w;
+    return m - left;
 }
 
-// Generic warp deletion (any number of keys): binary search in the sorted
-// group keys in global memory, `matched[run]` counts occurrences seen.
-__device__ __forceinline__ uint32_t warp_delete_global(const AdjView &view, const RowDesc &d, uint32_t u,
-                                                       const unsigned long long *keys, uint32_t gs, uint32_t ge,
-                                                       uint32_t *matched) {
+// Any number of keys: binary search in the sorted group keys in global
+// memory; matched[run] counts the occurrences of a run seen so far.
+__device__ __forceinline__ uint32_t warp_tomb_global(const AdjView &view, const RowDesc &d, uint32_t u,
+                                                     const unsigned long long *keys, uint32_t gs, uint32_t ge,
+                                                     uint32_t *matched) {
     const uint32_t lane = lane_id();
     const unsigned long long uhi = static_cast<unsigned long long>(u) << kKeyShift;
-    uint32_t w = 0;
-    for (uint32_t base = 0; base < d.deg; base += 32u) {
+    uint32_t left = ge - gs, done = 0;
+    for (uint32_t base = 0; base < d.len && left; base += 32u) {
         const uint32_t k = base + lane;
-        const bool valid = k < d.deg;
-        const uint32_t x = valid ? *view.at(d.off + k) : 0u;
+        const bool valid = k < d.len;
+        const uint32_t x = valid ? *view.at(d.off + k) : kTomb;
         uint32_t run = 0xFFFFFFFFu, req = 0;
-        const bool cand = valid && find_run(keys, gs, ge, uhi | x, run, req);
+        const bool cand = x != kTomb && find_run(keys, gs, ge, uhi | x, run, req);
         bool del = false;
         if (__ballot_sync(kFull, cand)) {
             const uint32_t peers = __match_any_sync(kFull, run);
@@ -264,25 +255,20 @@ __device__ __forceinline__ uint32_t warp_delete_global(const AdjView &view, cons
             if (cand && before == 0) matched[run] = seen + __popc(peers);
             __syncwarp();
         }
-        const bool keep = valid && !del;
-        const uint32_t km = __ballot_sync(kFull, keep);
-        const uint32_t pos = w + __popc(km & lanemask_lt());
-        __syncwarp();
-        if (keep && pos != k) write_slot(view, d.off + pos, x);
-        w += __popc(km);
+        const uint32_t dm = __ballot_sync(kFull, del);
+        if (del) write_slot(view, d.off + k, kTomb);
+        left -= __popc(dm);
+        done += __popc(dm);
     }
-    return w;
+    return done;
 }
 
 // Deletion phase, one warp per source group; rows above kWarpRowMax go to
 // the block path.  Launched with kMutWarps * 32 threads per block.
-constexpr int kMutWarps = 8;
-
-__global__ void __launch_bounds__(kMutWarps * 32) mutate_delete(AdjView view, RowDesc *desc, const unsigned long long *keys, uint32_t m,
-                              const uint32_t *groups, const uint32_t *gcount, uint32_t *matched, uint32_t *big,
-                              uint32_t *big_count, unsigned long long *stats, Status *st) {
-    __shared__ uint32_t stage_all[kMutWarps][128];
-    uint32_t *stage = stage_all[threadIdx.x >> 5];
+__global__ void __launch_bounds__(kMutWarps * 32)
+    mutate_delete(AdjView view, RowDesc *desc, const unsigned long long *keys, uint32_t m, const uint32_t *groups,
+                  const uint32_t *gcount, uint32_t *matched, uint32_t *big, uint32_t *big_count, uint32_t *compact,
+                  uint32_t *compact_count, unsigned long long *stats, Status *st) {
     const uint32_t lane = lane_id();
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t ng = *gcount;
@@ -292,16 +278,16 @@ __global__ void __launch_bounds__(kMutWarps * 32) mutate_delete(AdjView view, Ro
         const uint32_t ge = group_end(keys, m, gs);
         const uint32_t u = key_src(keys[gs]);
         const RowDesc d = desc[u];
-        if (d.deg > kWarpRowMax) {
+        if (d.len > kWarpRowMax) {
             if (lane == 0) big[atomicAdd(big_count, 1u)] = gs;
             continue;
         }
-        const uint32_t w = (ge - gs <= 32u) ? warp_delete_regs(view, d, keys, gs, ge - gs, stage)
-                                            : warp_delete_global(view, d, u, keys, gs, ge, matched);
+        const uint32_t done = (ge - gs <= 32u) ? warp_tomb_regs(view, d, keys, gs, ge - gs)
+                                               : warp_tomb_global(view, d, u, keys, gs, ge, matched);
         if (lane == 0) {
-            desc[u].deg = w;
-            removed += d.deg - w;
-            changed += (w != d.deg);
+            finish_row(desc, u, d, done, compact, compact_count);
+            removed += done;
+            changed += done != 0;
         }
     }
     if (lane == 0 && stats) {
@@ -310,26 +296,22 @@ __global__ void __launch_bounds__(kMutWarps * 32) mutate_delete(AdjView view, Ro
     }
 }
 
-// Deletion phase for rows above kWarpRowMax: one block per row, tiles of
-// kTpbMut x 8 entries (each thread two 16-byte loads), the group's keys and
-// matched counts in shared memory (up to kBigKeys keys; beyond that the
-// sorted keys and `matched` stay in global memory), a 4096-bit filter in
-// front of the key search, candidates resolved in position order by one
-// thread, and a block scan for the in-place compaction.
-constexpr int kTpbMut = 256;
+// Rows above kWarpRowMax: one block per row, tiles of kTpbMut x 8 slots
+// (two 16-byte loads per thread), the group's keys and matched counts in
+// shared memory (up to kBigKeys keys, beyond that in global memory), a
+// 4096-bit filter in front of the key search; candidates resolved in
+// position order by one thread; the scan stops once every request of the
+// row is satisfied.
 constexpr int kBigItems = 8;
 constexpr uint32_t kBigKeys = 2048;
 constexpr uint32_t kFilterBits = 4096;
 
 __device__ __forceinline__ uint32_t filter_hash(uint32_t x) { return (x * 0x9E3779B1u) >> 20; }  // 12 bits
 
-__global__ void __launch_bounds__(kTpbMut) mutate_delete_big(AdjView view, RowDesc *desc,
-                                                              const unsigned long long *keys, uint32_t m,
-                                                              const uint32_t *big, const uint32_t *big_count,
-                                                              uint32_t *matched, unsigned long long *stats,
-                                                              Status *st) {
-    using BlockScan = cub::BlockScan<uint32_t, kTpbMut>;
-    __shared__ typename BlockScan::TempStorage scan_tmp;
+__global__ void __launch_bounds__(kTpbMut)
+    mutate_delete_big(AdjView view, RowDesc *desc, const unsigned long long *keys, uint32_t m, const uint32_t *big,
+                      const uint32_t *big_count, uint32_t *matched, uint32_t *compact, uint32_t *compact_count,
+                      unsigned long long *stats, Status *st) {
     __shared__ uint32_t skey[kBigKeys];
     __shared__ uint32_t scount[kBigKeys];
     __shared__ uint32_t filter[kFilterBits / 32];
@@ -337,8 +319,8 @@ __global__ void __launch_bounds__(kTpbMut) mutate_delete_big(AdjView view, RowDe
     __shared__ uint8_t del_bits[kTpbMut];
     __shared__ uint16_t cand_run[kTpbMut * kBigItems];
     __shared__ uint32_t g_run[kTpbMut * kBigItems];
-    __shared__ uint32_t stage[kTpbMut * kBigItems];
-    __shared__ uint32_t any_cand;
+    __shared__ uint32_t cand_warp[kTpbMut / 32];
+    __shared__ uint32_t left;
     const uint32_t tid = threadIdx.x;
     const uint32_t nb = *big_count;
     for (uint32_t g = blockIdx.x; g < nb; g += gridDim.x) {
@@ -350,6 +332,7 @@ __global__ void __launch_bounds__(kTpbMut) mutate_delete_big(AdjView view, RowDe
         const RowDesc d = desc[u];
         const unsigned long long uhi = static_cast<unsigned long long>(u) << kKeyShift;
         for (uint32_t i = tid; i < kFilterBits / 32; i += kTpbMut) filter[i] = 0;
+        if (tid == 0) left = gm;
         __syncthreads();
         for (uint32_t j = tid; j < gm; j += kTpbMut) {
             const uint32_t x = key_low(keys[gs + j]);
@@ -361,26 +344,25 @@ __global__ void __launch_bounds__(kTpbMut) mutate_delete_big(AdjView view, RowDe
             atomicOr(&filter[h >> 5], 1u << (h & 31u));
         }
         __syncthreads();
-        uint32_t w = 0;
-        for (uint32_t base = 0; base < d.deg; base += kTpbMut * kBigItems) {
+        for (uint32_t base = 0; base < d.len; base += kTpbMut * kBigItems) {
             const uint32_t k0 = base + tid * kBigItems;
             uint32_t e[kBigItems];
 #pragma unroll
             for (int h = 0; h < kBigItems; h += 4) {
-                if (k0 + h < d.deg) {
+                if (k0 + h < d.len) {
                     const uint4 q = *reinterpret_cast<const uint4 *>(view.at(d.off + k0 + h));
                     e[h] = q.x;
                     e[h + 1] = q.y;
                     e[h + 2] = q.z;
                     e[h + 3] = q.w;
                 } else {
-                    e[h] = e[h + 1] = e[h + 2] = e[h + 3] = 0;
+                    e[h] = e[h + 1] = e[h + 2] = e[h + 3] = kTomb;
                 }
             }
             uint32_t cb = 0;
 #pragma unroll
             for (int s = 0; s < kBigItems; ++s) {
-                if (k0 + s >= d.deg) continue;
+                if (k0 + s >= d.len || e[s] == kTomb) continue;
                 const uint32_t h = filter_hash(e[s]);
                 if (!((filter[h >> 5] >> (h & 31u)) & 1u)) continue;
                 if (in_smem) {
@@ -406,63 +388,58 @@ __global__ void __launch_bounds__(kTpbMut) mutate_delete_big(AdjView view, RowDe
             }
             cand_bits[tid] = static_cast<uint8_t>(cb);
             del_bits[tid] = 0;
-            if (tid == 0) any_cand = 0;
-            __syncthreads();
-            if (cb) any_cand = 1;
-            __syncthreads();
-            if (any_cand) {
+            const uint32_t wmask = __ballot_sync(kFull, cb != 0);
+            if ((tid & 31u) == 0) cand_warp[tid >> 5] = wmask;
+            if (__syncthreads_or(cb != 0)) {
                 if (tid == 0) {
-                    for (uint32_t t = 0; t < kTpbMut; ++t) {
-                        uint32_t b = cand_bits[t];
-                        uint32_t dbits = 0;
-                        while (b) {
-                            const uint32_t s = __ffs(b) - 1;
-                            b &= b - 1;
-                            bool del;
-                            if (in_smem) {
-                                const uint32_t r = cand_run[t * kBigItems + s];
-                                uint32_t e2 = r + 1;
-                                while (e2 < gm && skey[e2] == skey[r]) ++e2;
-                                del = scount[r] < e2 - r;
-                                scount[r] += 1;
-                            } else {
-                                const uint32_t r = g_run[t * kBigItems + s];
-                                uint32_t e2 = r + 1;
-                                while (e2 < ge && keys[e2] == keys[r]) ++e2;
-                                del = matched[r] < e2 - r;
-                                matched[r] += 1;
+                    // Visit only the threads that hold candidates, in position order.
+                    uint32_t l = left;
+                    for (uint32_t wi = 0; wi < kTpbMut / 32; ++wi) {
+                        for (uint32_t tm = cand_warp[wi]; tm; tm &= tm - 1) {
+                            const uint32_t t = wi * 32 + __ffs(tm) - 1;
+                            uint32_t b = cand_bits[t];
+                            uint32_t dbits = 0;
+                            while (b) {
+                                const uint32_t s = __ffs(b) - 1;
+                                b &= b - 1;
+                                bool del;
+                                if (in_smem) {
+                                    const uint32_t r = cand_run[t * kBigItems + s];
+                                    uint32_t e2 = r + 1;
+                                    while (e2 < gm && skey[e2] == skey[r]) ++e2;
+                                    del = scount[r] < e2 - r;
+                                    scount[r] += 1;
+                                } else {
+                                    const uint32_t r = g_run[t * kBigItems + s];
+                                    uint32_t e2 = r + 1;
+                                    while (e2 < ge && keys[e2] == keys[r]) ++e2;
+                                    del = matched[r] < e2 - r;
+                                    matched[r] += 1;
+                                }
+                                if (del) {
+                                    dbits |= 1u << s;
+                                    --l;
+                                }
                             }
-                            if (del) dbits |= 1u << s;
+                            del_bits[t] = static_cast<uint8_t>(dbits);
                         }
-                        del_bits[t] = static_cast<uint8_t>(dbits);
                     }
+                    left = l;
                 }
                 __syncthreads();
-            }
-            const uint32_t db = del_bits[tid];
-            uint32_t kc = 0;
-#pragma unroll
-            for (int s = 0; s < kBigItems; ++s) kc += (k0 + s < d.deg && !((db >> s) & 1u)) ? 1u : 0u;
-            uint32_t prefix, total;
-            BlockScan(scan_tmp).ExclusiveSum(kc, prefix, total);
-            __syncthreads();
-            const uint32_t tile_valid = min(static_cast<uint32_t>(kTpbMut * kBigItems), d.deg - base);
-            if (w != base || total != tile_valid) {
-                // Stage the survivors, then store them with coalesced writes.
-                uint32_t pos = prefix;
+                const uint32_t db = del_bits[tid];
 #pragma unroll
                 for (int s = 0; s < kBigItems; ++s)
-                    if (k0 + s < d.deg && !((db >> s) & 1u)) stage[pos++] = e[s];
-                __syncthreads();
-                for (uint32_t i = tid; i < total; i += kTpbMut) write_slot(view, d.off + w + i, stage[i]);
+                    if ((db >> s) & 1u) write_slot(view, d.off + k0 + s, kTomb);
             }
-            w += total;
             __syncthreads();
+            if (left == 0) break;
         }
         if (tid == 0) {
-            desc[u].deg = w;
-            if (d.deg != w && stats) {
-                atomicAdd(&stats[kCntRemoved], static_cast<unsigned long long>(d.deg - w));
+            const uint32_t done = gm - left;
+            finish_row(desc, u, d, done, compact, compact_count);
+            if (done && stats) {
+                atomicAdd(&stats[kCntRemoved], static_cast<unsigned long long>(done));
                 atomicAdd(&stats[kCntChanged], 1ull);
             }
         }
@@ -470,7 +447,63 @@ __global__ void __launch_bounds__(kTpbMut) mutate_delete_big(AdjView view, RowDe
     }
 }
 
-// Addition plan: rows that outgrow their block get a class and a rank.
+// ---------------------------------------------------------------- compaction
+
+// Drop the tombstones of the queued rows in place (order kept).  One block
+// per row; tiles of kTpbMut x 8 slots, block scan, survivors staged in
+// shared memory and stored with coalesced writes.
+__global__ void __launch_bounds__(kTpbMut) compact_rows(AdjView view, RowDesc *desc, const uint32_t *list,
+                                                         const uint32_t *count) {
+    using BlockScan = cub::BlockScan<uint32_t, kTpbMut>;
+    __shared__ typename BlockScan::TempStorage scan_tmp;
+    __shared__ uint32_t stage[kTpbMut * kBigItems];
+    const uint32_t tid = threadIdx.x;
+    const uint32_t nc = *count;
+    for (uint32_t c = blockIdx.x; c < nc; c += gridDim.x) {
+        const uint32_t u = list[c];
+        const RowDesc d = desc[u];
+        uint32_t w = 0;
+        for (uint32_t base = 0; base < d.len; base += kTpbMut * kBigItems) {
+            const uint32_t k0 = base + tid * kBigItems;
+            uint32_t e[kBigItems];
+#pragma unroll
+            for (int h = 0; h < kBigItems; h += 4) {
+                if (k0 + h < d.len) {
+                    const uint4 q = *reinterpret_cast<const uint4 *>(view.at(d.off + k0 + h));
+                    e[h] = q.x;
+                    e[h + 1] = q.y;
+                    e[h + 2] = q.z;
+                    e[h + 3] = q.w;
+                } else {
+                    e[h] = e[h + 1] = e[h + 2] = e[h + 3] = kTomb;
+                }
+            }
+            uint32_t kc = 0;
+#pragma unroll
+            for (int s = 0; s < kBigItems; ++s) kc += (k0 + s < d.len && e[s] != kTomb) ? 1u : 0u;
+            uint32_t prefix, total;
+            BlockScan(scan_tmp).ExclusiveSum(kc, prefix, total);
+            uint32_t pos = prefix;
+#pragma unroll
+            for (int s = 0; s < kBigItems; ++s)
+                if (k0 + s < d.len && e[s] != kTomb) stage[pos++] = e[s];
+            __syncthreads();  // every load of this tile is done before any store
+            const uint32_t tile_valid = min(static_cast<uint32_t>(kTpbMut * kBigItems), d.len - base);
+            if (w != base || total != tile_valid)
+                for (uint32_t i = tid; i < total; i += kTpbMut) write_slot(view, d.off + w + i, stage[i]);
+            w += total;
+            __syncthreads();
+        }
+        if (tid == 0) desc[u] = RowDesc{d.off, w, rd_meta(rd_cls(d), 0)};
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- addition
+
+// Addition plan: rows that outgrow their block get a class (sized for the
+// live entries plus the additions, since relocation drops tombstones) and a
+// rank in that class.
 __global__ void plan_add(const RowDesc *desc, const unsigned long long *keys, uint32_t m, const uint32_t *groups,
                          const uint32_t *gcount, unsigned long long *plan, ArenaAlloc *al) {
     const uint32_t ng = *gcount;
@@ -478,12 +511,13 @@ __global__ void plan_add(const RowDesc *desc, const unsigned long long *keys, ui
         const uint32_t gs = groups[g];
         const uint32_t ge = group_end(keys, m, gs);
         const RowDesc d = desc[key_src(keys[gs])];
-        const unsigned long long nd = static_cast<unsigned long long>(d.deg) + (ge - gs);
+        const unsigned long long used = static_cast<unsigned long long>(d.len) + (ge - gs);
+        const unsigned long long live = static_cast<unsigned long long>(rd_live(d)) + (ge - gs);
         unsigned long long p = kKeyNone;
-        if (nd > 0xFFFFFFFFull) {
+        if (live > 0xFFFFFFFFull) {
             p = kKeyNone - 1;  // degree overflow, reported by the apply kernel
-        } else if (d.cls == 0 || nd > (1ull << d.cls)) {
-            const uint32_t cls = class_for(static_cast<uint32_t>(nd));
+        } else if (rd_cls(d) == 0 || used > (1ull << rd_cls(d))) {
+            const uint32_t cls = class_for(static_cast<uint32_t>(live));
             const uint32_t rank = atomicAdd(&al->demand[cls], 1u);
             p = (static_cast<unsigned long long>(cls) << 32) | rank;
         }
@@ -533,7 +567,7 @@ __global__ void alloc_classes(ArenaAlloc *al, Status *st) {
 
 // Addition phase, one warp per group (rows above kWarpRowMax that must move
 // go to the block path).  `vals` is add_v for the forward arena and add_u
-// for the reverse arena.
+// for the reverse arena.  A moving row is copied without its tombstones.
 __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long *keys, uint32_t m,
                            const uint32_t *groups, const uint32_t *gcount, const unsigned long long *plan,
                            const ArenaAlloc *al, const uint32_t *vals, uint32_t *big, uint32_t *big_count,
@@ -554,20 +588,28 @@ __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long
         const uint32_t u = key_src(keys[gs]);
         const RowDesc d = desc[u];
         const uint32_t a = ge - gs;
-        unsigned long long off = d.off;
-        uint32_t cls = d.cls;
-        if (p != kKeyNone) {
-            if (d.deg > kWarpRowMax) {
+        if (p == kKeyNone) {
+            for (uint32_t j = lane; j < a; j += 32u) write_slot(view, d.off + d.len + j, vals[key_low(keys[gs + j])]);
+            if (lane == 0) desc[u] = RowDesc{d.off, d.len + a, d.meta};
+        } else {
+            if (d.len > kWarpRowMax) {
                 if (lane == 0) big[atomicAdd(big_count, 1u)] = g;
                 continue;
             }
-            cls = static_cast<uint32_t>(p >> 32);
-            off = alloc_offset(al, cls, static_cast<uint32_t>(p));
-            for (uint32_t k = lane; k < d.deg; k += 32u) write_slot(view, off + k, *view.at(d.off + k));
+            const uint32_t cls = static_cast<uint32_t>(p >> 32);
+            const unsigned long long off = alloc_offset(al, cls, static_cast<uint32_t>(p));
+            uint32_t w = 0;
+            for (uint32_t base = 0; base < d.len; base += 32u) {
+                const uint32_t k = base + lane;
+                const uint32_t x = k < d.len ? *view.at(d.off + k) : kTomb;
+                const uint32_t km = __ballot_sync(kFull, x != kTomb);
+                if (x != kTomb) write_slot(view, off + w + __popc(km & lanemask_lt()), x);
+                w += __popc(km);
+            }
+            for (uint32_t j = lane; j < a; j += 32u) write_slot(view, off + w + j, vals[key_low(keys[gs + j])]);
+            if (lane == 0) desc[u] = RowDesc{off, w + a, rd_meta(cls, 0)};
             moved += 1;
         }
-        for (uint32_t j = lane; j < a; j += 32u) write_slot(view, off + d.deg + j, vals[key_low(keys[gs + j])]);
-        if (lane == 0) desc[u] = RowDesc{off, d.deg + a, cls};
         changed += 1;
     }
     if (lane == 0 && stats) {
@@ -576,12 +618,12 @@ __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long
     }
 }
 
-__global__ void __launch_bounds__(kTpbMut) mutate_add_big(AdjView view, RowDesc *desc,
-                                                          const unsigned long long *keys, uint32_t m,
-                                                          const uint32_t *groups, const unsigned long long *plan,
-                                                          const ArenaAlloc *al, const uint32_t *vals,
-                                                          const uint32_t *big, const uint32_t *big_count,
-                                                          unsigned long long *stats, Status *st) {
+__global__ void __launch_bounds__(kTpbMut)
+    mutate_add_big(AdjView view, RowDesc *desc, const unsigned long long *keys, uint32_t m, const uint32_t *groups,
+                   const unsigned long long *plan, const ArenaAlloc *al, const uint32_t *vals, const uint32_t *big,
+                   const uint32_t *big_count, unsigned long long *stats, Status *st) {
+    using BlockScan = cub::BlockScan<uint32_t, kTpbMut>;
+    __shared__ typename BlockScan::TempStorage scan_tmp;
     if (ld_volatile(&st->err) & kErrArena) return;
     const uint32_t nb = *big_count;
     for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
@@ -594,11 +636,20 @@ __global__ void __launch_bounds__(kTpbMut) mutate_add_big(AdjView view, RowDesc 
         const uint32_t a = ge - gs;
         const uint32_t cls = static_cast<uint32_t>(p >> 32);
         const unsigned long long off = alloc_offset(al, cls, static_cast<uint32_t>(p));
-        for (uint32_t k = threadIdx.x; k < d.deg; k += kTpbMut) write_slot(view, off + k, *view.at(d.off + k));
-        for (uint32_t j = threadIdx.x; j < a; j += kTpbMut) write_slot(view, off + d.deg + j, vals[key_low(keys[gs + j])]);
+        uint32_t w = 0;
+        for (uint32_t base = 0; base < d.len; base += kTpbMut) {
+            const uint32_t k = base + threadIdx.x;
+            const uint32_t x = k < d.len ? *view.at(d.off + k) : kTomb;
+            uint32_t prefix, total;
+            BlockScan(scan_tmp).ExclusiveSum(x != kTomb ? 1u : 0u, prefix, total);
+            if (x != kTomb) write_slot(view, off + w + prefix, x);
+            w += total;
+            __syncthreads();
+        }
+        for (uint32_t j = threadIdx.x; j < a; j += kTpbMut) write_slot(view, off + w + j, vals[key_low(keys[gs + j])]);
         __syncthreads();
         if (threadIdx.x == 0) {
-            desc[u] = RowDesc{off, d.deg + a, cls};
+            desc[u] = RowDesc{off, w + a, rd_meta(cls, 0)};
             if (stats) {
                 atomicAdd(&stats[kCntChanged], 1ull);
                 atomicAdd(&stats[kCntRelocated], 1ull);

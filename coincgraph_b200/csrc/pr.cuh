@@ -129,22 +129,22 @@ __global__ void __launch_bounds__(kTpbPr) pr_converge(AdjView fwd, PrArrays<T> a
             if (pr_abs(rv) > eps) {
                 rank_add(a, v, rv);
                 a.res[v] = T(0);
-                const uint32_t deg = fwd.desc[v].deg;
+                const uint32_t deg = rd_live(fwd.desc[v]);  // out-degree: live entries only
                 if (deg) c = alpha * rv / static_cast<T>(deg);
             }
             a.contrib[i] = c;
         }
         if (!grid_barrier(st)) break;
         PrPushOp<T> op{a.res, a.queued, a.contrib, eps, (r & 1) ? a.q0 : a.q1, a.cnt + ((r + 1) % 3), a.cap, st};
-        for (uint32_t base = blockIdx.x * kTpbPr; base < n_in; base += gridDim.x * kTpbPr) {
-            const uint32_t i = base + threadIdx.x;
+        for (uint32_t base = 0; base < n_in; base += gridDim.x * kTpbPr) {
+            const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
             bool has = i < n_in;
             uint32_t v = 0, deg = 0;
             uint64_t off = 0;
             if (has) {
                 v = __ldcg(in + i);
                 const RowDesc d = fwd.desc[v];
-                deg = d.deg;
+                deg = d.len;
                 off = d.off;
                 has = deg > 0 && __ldcg(a.contrib + i) != T(0);
                 if (has && seg_hot) atomicAdd(seg_hot + (off >> kSegShift), 1u);
@@ -205,7 +205,7 @@ __global__ void pr_amend_contrib(const RowDesc *desc, PrArrays<T> a, const uint3
     const T alpha = sizeof(T) == 4 ? T(kAlphaF) : T(kAlphaD);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t s = list[i];
-        const uint32_t deg = desc[s].deg;
+        const uint32_t deg = rd_live(desc[s]);
         contrib[i] = deg ? sign * alpha * rank_value(a, s) / static_cast<T>(deg) : T(0);
     }
 }
@@ -218,15 +218,15 @@ __global__ void __launch_bounds__(kTpbPr) pr_amend_scatter(AdjView fwd, PrArrays
     ExpandCounters cnt;
     const uint32_t n = *count;
     PrPushOp<T> op{a.res, a.queued, contrib, eps, a.q0, a.cnt, a.cap, st};
-    for (uint32_t base = blockIdx.x * kTpbPr; base < n; base += gridDim.x * kTpbPr) {
-        const uint32_t i = base + threadIdx.x;
+    for (uint32_t base = 0; base < n; base += gridDim.x * kTpbPr) {
+        const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
         bool has = i < n;
         uint32_t s = 0, deg = 0;
         uint64_t off = 0;
         if (has) {
             s = list[i];
             const RowDesc d = fwd.desc[s];
-            deg = d.deg;
+            deg = d.len;
             off = d.off;
             has = deg > 0 && contrib[i] != T(0);
         }

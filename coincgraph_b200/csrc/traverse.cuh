@@ -132,9 +132,18 @@ struct PullOp {
 // Persistent push closure (cooperative launch).  Replaces RunExactGpuClosure
 // (framework.cuh:342-454) and the Start loop (:1151-1182): waves of relaxation
 // until no vertex improves, with bounded grid barriers and a round bound.
+// Rows of at least kSplitDeg entries met in a round go to `big` (three round
+// counters, as for the frontier) and are expanded by the whole grid after a
+// barrier; rounds without such rows keep a single barrier.
+struct BigList {
+    BigRow *rows;
+    uint32_t *cnt;  // 3 counters
+    uint32_t cap;
+};
+
 template <int A>
 __global__ void __launch_bounds__(kTpb) push_closure(AdjView fwd, unsigned long long *state, uint32_t *qstamp,
-                                                     TagState *tags, Frontier fr, uint32_t max_rounds,
+                                                     TagState *tags, Frontier fr, BigList big, uint32_t max_rounds,
                                                      uint32_t *seg_hot, Status *st) {
     __shared__ ExpandSmem<kTpb> sm;
     ExpandCounters cnt;
@@ -148,11 +157,17 @@ __global__ void __launch_bounds__(kTpb) push_closure(AdjView fwd, unsigned long 
             if (blockIdx.x == 0 && threadIdx.x == 0) set_error(st, kErrRounds, r);
             break;
         }
-        if (blockIdx.x == 0 && threadIdx.x == 0) fr.cnt[(r + 2) % 3] = 0;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            fr.cnt[(r + 2) % 3] = 0;
+            big.cnt[(r + 2) % 3] = 0;
+        }
         const uint32_t *in = (r & 1) ? fr.q1 : fr.q0;
         PushOp<A> op{state, qstamp, tag0 + r, (r & 1) ? fr.q0 : fr.q1, fr.cnt + ((r + 1) % 3), fr.cap, st};
-        for (uint32_t base = blockIdx.x * kTpb; base < n_in; base += gridDim.x * kTpb) {
-            const uint32_t i = base + threadIdx.x;
+        const Defer df{big.rows, big.cnt + (r % 3), big.cap};
+        // Item i goes to block i mod gridDim.x, so small frontiers still
+        // spread over the whole grid.
+        for (uint32_t base = 0; base < n_in; base += gridDim.x * kTpb) {
+            const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
             bool has = i < n_in;
             uint32_t x = 0, dx = 0, deg = 0;
             uint64_t off = 0;
@@ -160,14 +175,19 @@ __global__ void __launch_bounds__(kTpb) push_closure(AdjView fwd, unsigned long 
                 x = __ldcg(in + i);
                 dx = val_of(__ldcg(state + x));
                 const RowDesc d = fwd.desc[x];
-                deg = d.deg;
+                deg = d.len;
                 off = d.off;
                 has = dx != kInf && deg > 0;
                 if (has && seg_hot) atomicAdd(seg_hot + (off >> kSegShift), 1u);
             }
-            expand_rows<kTpb>(fwd, has, x, dx, off, deg, op, sm, cnt);
+            expand_rows<kTpb>(fwd, has, x, dx, off, deg, op, sm, cnt, df);
         }
         if (!grid_barrier(st)) break;
+        const uint32_t nbig = min(ld_volatile(big.cnt + (r % 3)), big.cap);
+        if (nbig) {
+            expand_deferred<kTpb>(fwd, big.rows, nbig, op, cnt);
+            if (!grid_barrier(st)) break;
+        }
     }
     flush_counters(st, cnt, kCntPush);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -182,8 +202,8 @@ __global__ void __launch_bounds__(kTpb) push_closure(AdjView fwd, unsigned long 
 template <int A>
 __global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long long *state, uint32_t *aff_stamp,
                                                       uint32_t epoch, uint32_t *list, uint32_t *cnt3,
-                                                      uint32_t cap, uint32_t max_rounds, uint32_t *aff_total,
-                                                      Status *st) {
+                                                      uint32_t cap, BigList big, uint32_t max_rounds,
+                                                      uint32_t *aff_total, Status *st) {
     __shared__ ExpandSmem<kTpb> sm;
     ExpandCounters c;
     uint32_t lo = 0, hi = ld_volatile(cnt3 + 0);
@@ -194,11 +214,15 @@ __global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long
             if (blockIdx.x == 0 && threadIdx.x == 0) set_error(st, kErrRounds, r);
             break;
         }
-        if (blockIdx.x == 0 && threadIdx.x == 0) cnt3[(r + 2) % 3] = 0;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            cnt3[(r + 2) % 3] = 0;
+            big.cnt[(r + 2) % 3] = 0;
+        }
         InvalOp<A> op{state, aff_stamp, epoch, list + hi, cnt3 + ((r + 1) % 3), cap > hi ? cap - hi : 0u, st};
+        const Defer df{big.rows, big.cnt + (r % 3), big.cap};
         const uint32_t n_in = hi - lo;
-        for (uint32_t base = blockIdx.x * kTpb; base < n_in; base += gridDim.x * kTpb) {
-            const uint32_t i = base + threadIdx.x;
+        for (uint32_t base = 0; base < n_in; base += gridDim.x * kTpb) {
+            const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
             bool has = i < n_in;
             uint32_t x = 0, px = 0, deg = 0;
             uint64_t off = 0;
@@ -206,13 +230,18 @@ __global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long
                 x = __ldcg(list + lo + i);
                 px = (A == kCc) ? val_of(__ldcg(state + x)) : x;
                 const RowDesc d = fwd.desc[x];
-                deg = d.deg;
+                deg = d.len;
                 off = d.off;
                 has = deg > 0;
             }
-            expand_rows<kTpb>(fwd, has, x, px, off, deg, op, sm, c);
+            expand_rows<kTpb>(fwd, has, x, px, off, deg, op, sm, c, df);
         }
         if (!grid_barrier(st)) break;
+        const uint32_t nbig = min(ld_volatile(big.cnt + (r % 3)), big.cap);
+        if (nbig) {
+            expand_deferred<kTpb>(fwd, big.rows, nbig, op, c);
+            if (!grid_barrier(st)) break;
+        }
         lo = hi;
         hi = hi + ld_volatile(cnt3 + ((r + 1) % 3));
     }
@@ -265,25 +294,36 @@ __global__ void reset_affected(const uint32_t *list, const uint32_t *total, unsi
 template <int A>
 __global__ void __launch_bounds__(kTpb) pull_repair(AdjView rev, unsigned long long *state, const uint32_t *aff_stamp,
                                                     uint32_t epoch, const uint32_t *list, const uint32_t *total,
-                                                    Status *st) {
+                                                    BigList big, Status *st) {
     __shared__ ExpandSmem<kTpb> sm;
     ExpandCounters c;
     const uint32_t n = *total;
     PullOp<A> op{state, aff_stamp, epoch};
-    for (uint32_t base = blockIdx.x * kTpb; base < n; base += gridDim.x * kTpb) {
-        const uint32_t i = base + threadIdx.x;
+    const Defer df{big.rows, big.cnt, big.cap};
+    for (uint32_t base = 0; base < n; base += gridDim.x * kTpb) {
+        const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
         bool has = i < n;
         uint32_t v = 0, deg = 0;
         uint64_t off = 0;
         if (has) {
             v = list[i];
             const RowDesc d = rev.desc[v];
-            deg = d.deg;
+            deg = d.len;
             off = d.off;
             has = deg > 0;
         }
-        expand_rows<kTpb>(rev, has, v, 0u, off, deg, op, sm, c);
+        expand_rows<kTpb>(rev, has, v, 0u, off, deg, op, sm, c, df);
     }
+    flush_counters(st, c, kCntPull);
+}
+
+// The in-rows that pull_repair deferred, expanded by the whole grid.
+template <int A>
+__global__ void __launch_bounds__(kTpb) pull_deferred(AdjView rev, unsigned long long *state, const uint32_t *aff_stamp,
+                                                      uint32_t epoch, BigList big, Status *st) {
+    ExpandCounters c;
+    PullOp<A> op{state, aff_stamp, epoch};
+    expand_deferred<kTpb>(rev, big.rows, min(*big.cnt, big.cap), op, c);
     flush_counters(st, c, kCntPull);
 }
 
@@ -350,7 +390,7 @@ __global__ void enqueue_all_nonempty(const RowDesc *desc, uint32_t n, Frontier f
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t rounded = (n + 31u) & ~31u;
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < rounded; v += stride) {
-        const bool want = v < n && desc[v].deg > 0;
+        const bool want = v < n && rd_live(desc[v]) > 0;
         warp_enqueue(want, v, fr.q0, fr.cnt, fr.cap, st);
     }
 }

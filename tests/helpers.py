@@ -88,8 +88,12 @@ def big_row_case() -> Case:
     """Rows above the warp path (5000 entries) and above one segment (20000)."""
     rng = np.random.default_rng(7)
     n = 30000
-    src = np.concatenate([np.zeros(20000, np.int64), np.ones(5000, np.int64), rng.integers(0, n, 30000)])
-    dst = np.concatenate([rng.integers(2, n, 20000), rng.integers(2, n, 5000), rng.integers(0, n, 30000)])
+    # vertex 5 has 6000 in-edges and its parent edge (0, 5) is deleted in
+    # batch 0, so the pull repair meets an in-row above the split threshold
+    src = np.concatenate([np.zeros(20000, np.int64), np.ones(5000, np.int64), rng.integers(0, n, 30000),
+                          np.arange(100, 6100), [0]])
+    dst = np.concatenate([rng.integers(6, n, 20000), rng.integers(2, n, 5000), rng.integers(0, n, 30000),
+                          np.full(6000, 5), [5]])
     xadj, adj = _csr_from_edges(n, src, dst)
     row0 = adj[int(xadj[0]):int(xadj[1])]
     row1 = adj[int(xadj[1]):int(xadj[2])]
@@ -97,8 +101,10 @@ def big_row_case() -> Case:
     for k in range(3):
         pick0 = row0[rng.integers(0, len(row0), 50)]
         pick1 = row1[rng.integers(0, len(row1), 20)]
-        du = np.concatenate([np.zeros(50, np.uint32), np.ones(20, np.uint32), rng.integers(0, n, 30).astype(np.uint32)])
-        dv = np.concatenate([pick0, pick1, rng.integers(0, n, 30)]).astype(np.uint32)
+        extra = 1 if k == 0 else 0
+        du = np.concatenate([np.zeros(50, np.uint32), np.ones(20, np.uint32), rng.integers(0, n, 30).astype(np.uint32),
+                             np.zeros(extra, np.uint32)])
+        dv = np.concatenate([pick0, pick1, rng.integers(0, n, 30), np.full(extra, 5)]).astype(np.uint32)
         # batch 1 pushes row 0 past its 32768-slot block and row 1 past 8192
         au = np.concatenate([np.zeros(13000 * (k == 1), np.uint32), np.ones(4000 * (k == 1), np.uint32),
                              rng.integers(0, n, 100).astype(np.uint32)])
