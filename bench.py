@@ -346,7 +346,7 @@ def run_ours(args):
     hbm_peak, peak_kind = load_peaks()
     link_peak = link_peak_gbs(torch, dev)
     stages = {}
-    for name in ("group", "mutate", "mutate_rev", "seed", "inval", "pull", "push"):
+    for name in ("group", "mutate", "mutate_rev", "add", "add_rev", "seed", "inval", "pull", "push"):
         stages[name] = {"ms_per_batch": prof[name]["ms"] / args.steps, "launches": prof[name]["launches"]}
     trav = {n: stage_roofline(prof[n], hbm_peak, link_peak) for n in ("inval", "pull", "push")}
     dominant = max(("push", "inval", "pull"), key=lambda n: prof[n]["ms"])

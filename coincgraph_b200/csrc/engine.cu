@@ -870,7 +870,7 @@ struct cig_handle {
         CK(cudaMemsetAsync(bcount, 0, sizeof(uint32_t), stream));
         launch(find_groups, grid_for(na), 256, sorted, m, groups, gcount);
         prof_end(p);
-        p = prof_begin(forward ? CIG_STAGE_MUTATE : CIG_STAGE_MUTATE_REV);
+        p = prof_begin(forward ? CIG_STAGE_ADD : CIG_STAGE_ADD_REV);
         launch(plan_add, persistent_grid(), 256, A.desc, sorted, m, groups, gcount, plan, A.alloc);
         launch(alloc_classes, 1, 64, A.alloc, status);
         unsigned long long *stats = with_stats ? status->counters : nullptr;

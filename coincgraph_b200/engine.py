@@ -88,7 +88,7 @@ class GraphInfo(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
-STAGES = ["group", "mutate", "seed", "inval", "pull", "push", "pr", "cache", "mutate_rev"]
+STAGES = ["group", "mutate", "seed", "inval", "pull", "push", "pr", "cache", "mutate_rev", "add", "add_rev"]
 
 
 class StageProfile(ctypes.Structure):

@@ -134,6 +134,29 @@ def updates(graph_handle, del_sizes, add_sizes, seed: int, symmetric: bool = Fal
     return UpdateStream(du[:nd], dv[:nd], au[:na], av[:na], del_off, add_off)
 
 
+def write_graph_txt(path: str, g: Graph, weights: bool = True) -> None:
+    """Write `u v [w]` lines (the reference's market_big format, weight
+    (u+v)%128 as its --weight_num=1 synthesises it)."""
+    src = np.repeat(np.arange(g.n, dtype=np.uint64), np.diff(g.xadj).astype(np.int64))
+    dst = g.adj.astype(np.uint64)
+    cols = [src, dst] + ([(src + dst) % 128] if weights else [])
+    np.savetxt(path, np.stack(cols, axis=1), fmt="%d", delimiter=" ")
+
+
+def write_updates_txt(update_path: str, size_path: str, ups: UpdateStream) -> None:
+    """Write updates.txt (`d u v w` lines then `a u v w` lines per batch) and
+    batches.txt (`adds dels` per batch), the reference's Loader format."""
+    with open(update_path, "w") as f:
+        for i in range(ups.batches):
+            du, dv, au, av = ups.batch(i)
+            for kind, us, vs in (("d", du, dv), ("a", au, av)):
+                w = (us.astype(np.uint64) + vs.astype(np.uint64)) % 128
+                f.writelines(f"{kind} {u} {v} {x}\n" for u, v, x in zip(us.tolist(), vs.tolist(), w.tolist()))
+    with open(size_path, "w") as f:
+        for i in range(ups.batches):
+            f.write(f"{int(ups.add_off[i + 1] - ups.add_off[i])} {int(ups.del_off[i + 1] - ups.del_off[i])}\n")
+
+
 def graph_from_edges(n: int, src, dst) -> Graph:
     """CSR from an edge list, rows in input (file) order, as the reference's
     market_big reader builds them (src/utils/parser.cpp:292-402)."""

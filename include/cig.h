@@ -185,7 +185,9 @@ enum {
     CIG_STAGE_PR = 6,     /* PageRank amend + converge */
     CIG_STAGE_CACHE = 7,  /* edge-cache maintenance */
     CIG_STAGE_MUTATE_REV = 8, /* reverse (in-edge) rows */
-    CIG_STAGE_COUNT = 9
+    CIG_STAGE_ADD = 9,        /* forward rows, addition phase (MUTATE is then the deletion phase) */
+    CIG_STAGE_ADD_REV = 10,   /* reverse rows, addition phase */
+    CIG_STAGE_COUNT = 11
 };
 
 typedef struct {
