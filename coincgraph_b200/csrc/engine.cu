@@ -22,6 +22,7 @@
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include "../../include/cig.h"
 #include "common.cuh"
@@ -175,6 +176,7 @@ enum SmallIdx : int {
     kFinalRound = 12,
     kBigRows = 13,  // 3 counters of deferred hub rows
     kCompactCount = 16,
+    kOrderedCount = 17,
     kSmallCount = 20
 };
 
@@ -258,6 +260,11 @@ struct cig_handle {
     unsigned long long *pf = nullptr, *prr = nullptr;
     uint32_t *touched = nullptr;
     uint32_t *compact = nullptr;  // rows queued for tombstone compaction
+    // flat deletion: per-group chunk counts, their inclusive prefix sum, the
+    // groups left to the ordered kernels, first match per key
+    uint32_t *chunks = nullptr, *chunk_end = nullptr, *ordered = nullptr, *firstpos = nullptr;
+    // group building: head flags, their exclusive scan, group ends per direction
+    uint32_t *gflags = nullptr, *gpos = nullptr, *gendf = nullptr, *gendr = nullptr;
     void *cub = nullptr;
     size_t cub_bytes = 0;
     uint32_t *stage = nullptr;  // pinned staging for host update arrays (4 * bcap)
@@ -495,6 +502,14 @@ struct cig_handle {
         dfree(prr);
         dfree(touched);
         dfree(compact);
+        dfree(chunks);
+        dfree(chunk_end);
+        dfree(ordered);
+        dfree(firstpos);
+        dfree(gflags);
+        dfree(gpos);
+        dfree(gendf);
+        dfree(gendr);
         dfree(cub);
         if (stage) cudaFreeHost(stage);
         stage = nullptr;
@@ -525,6 +540,14 @@ struct cig_handle {
         dmalloc(prr, cap);
         dmalloc(touched, 2 * cap);
         dmalloc(compact, cap);
+        dmalloc(chunks, cap);
+        dmalloc(chunk_end, cap);
+        dmalloc(ordered, cap);
+        dmalloc(firstpos, cap);
+        dmalloc(gflags, cap);
+        dmalloc(gpos, cap);
+        dmalloc(gendf, cap);
+        dmalloc(gendr, cap);
         if (opt.algo == CIG_PR) {
             dfree(pr_amend);
             CK(cudaMalloc(&pr_amend, 2 * cap * (pr64 ? sizeof(double) : sizeof(float))));
@@ -532,6 +555,11 @@ struct cig_handle {
         cub::DoubleBuffer<unsigned long long> db(kf, t1);
         size_t bytes = 0;
         CK(cub::DeviceRadixSort::SortKeys(nullptr, bytes, db, static_cast<int>(cap), 0, 64, stream));
+        size_t scan_bytes = 0;
+        CK(cub::DeviceScan::InclusiveSum(nullptr, scan_bytes, chunks, chunk_end, static_cast<int>(cap), stream));
+        bytes = std::max(bytes, scan_bytes);
+        CK(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, gflags, gpos, static_cast<int>(cap), stream));
+        bytes = std::max(bytes, scan_bytes);
         cub_bytes = bytes;
         CK(cudaMalloc(&cub, std::max<size_t>(bytes, 16)));
         CK(cudaHostAlloc(reinterpret_cast<void **>(&stage), 4 * cap * sizeof(uint32_t), cudaHostAllocDefault));
@@ -813,6 +841,19 @@ struct cig_handle {
         mutate_add_arena(fwd, d_au, d_av, na, true, with_stats);
     }
 
+    // Source groups of a sorted key array, in key order (flags, exclusive
+    // scan, scatter): group g spans keys [start[g], end[g]).
+    Groups build_groups(const unsigned long long *sorted, uint64_t count, uint32_t *start, uint32_t *end,
+                        uint32_t *gcount) {
+        const uint32_t m = static_cast<uint32_t>(count);
+        CK(cudaMemsetAsync(gcount, 0, sizeof(uint32_t), stream));
+        launch(group_flags, grid_for(count), 256, sorted, m, gflags);
+        size_t bytes = cub_bytes;
+        CK(cub::DeviceScan::ExclusiveSum(cub, bytes, gflags, gpos, static_cast<int>(count), stream));
+        launch(group_scatter, grid_for(count), 256, sorted, m, gflags, gpos, start, end, gcount);
+        return Groups{start, end, gcount};
+    }
+
     void mutate_delete_arena(DevArena &A, const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd, bool forward,
                              bool with_stats) {
         if (nd == 0) return;
@@ -831,18 +872,31 @@ struct cig_handle {
             check_launch();
         }
         unsigned long long *sorted = sort_keys(keys, tmp, nd);
-        CK(cudaMemsetAsync(gcount, 0, sizeof(uint32_t), stream));
         CK(cudaMemsetAsync(bcount, 0, sizeof(uint32_t), stream));
         CK(cudaMemsetAsync(matched, 0, nd * sizeof(uint32_t), stream));
-        launch(find_groups, grid_for(nd), 256, sorted, m, groups, gcount);
+        const Groups grp = build_groups(sorted, nd, groups, forward ? gendf : gendr, gcount);
         prof_end(p);
         p = prof_begin(forward ? CIG_STAGE_MUTATE : CIG_STAGE_MUTATE_REV);
         unsigned long long *stats = with_stats ? status->counters : nullptr;
         uint32_t *ccount = small + kCompactCount;
+        uint32_t *ocount = small + kOrderedCount;
         CK(cudaMemsetAsync(ccount, 0, sizeof(uint32_t), stream));
-        launch(mutate_delete, persistent_grid(), kMutWarps * 32, A.view(), A.desc, sorted, m, groups, gcount,
+        CK(cudaMemsetAsync(ocount, 0, sizeof(uint32_t), stream));
+        CK(cudaMemsetAsync(chunks, 0, nd * sizeof(uint32_t), stream));
+        CK(cudaMemsetAsync(firstpos, 0xFF, nd * sizeof(uint32_t), stream));
+        // Flat path: rows whose deletion requests are all distinct.
+        launch(del_classify, persistent_grid(), 256, A.desc, sorted, grp, chunks, ordered, ocount);
+        {
+            size_t bytes = cub_bytes;
+            CK(cub::DeviceScan::InclusiveSum(cub, bytes, chunks, chunk_end, static_cast<int>(nd), stream));
+        }
+        launch(del_scan, persistent_grid(), kMutWarps * 32, A.view(), A.desc, sorted, grp, chunk_end, m, firstpos);
+        launch(del_apply, grid_for(nd), 256, A.view(), A.desc, sorted, m, firstpos, stats);
+        launch(del_finish, persistent_grid(), 256, A.desc, sorted, grp, chunks, firstpos, compact, ccount, stats);
+        // Ordered path: rows with repeated requests for a destination.
+        launch(mutate_delete, persistent_grid(), kMutWarps * 32, A.view(), A.desc, sorted, grp, ordered, ocount,
                matched, big, bcount, compact, ccount, stats, status);
-        launch(mutate_delete_big, sms * 4, kTpbMut, A.view(), A.desc, sorted, m, big, bcount, matched, compact,
+        launch(mutate_delete_big, sms * 4, kTpbMut, A.view(), A.desc, sorted, grp, big, bcount, matched, compact,
                ccount, stats, status);
         launch(compact_rows, sms * 4, kTpbMut, A.view(), A.desc, compact, ccount);
         prof_end(p);
@@ -866,19 +920,18 @@ struct cig_handle {
             check_launch();
         }
         unsigned long long *sorted = sort_keys(keys, tmp, na);
-        CK(cudaMemsetAsync(gcount, 0, sizeof(uint32_t), stream));
         CK(cudaMemsetAsync(bcount, 0, sizeof(uint32_t), stream));
-        launch(find_groups, grid_for(na), 256, sorted, m, groups, gcount);
+        const Groups grp = build_groups(sorted, na, groups, forward ? gendf : gendr, gcount);
         prof_end(p);
         p = prof_begin(forward ? CIG_STAGE_ADD : CIG_STAGE_ADD_REV);
-        launch(plan_add, persistent_grid(), 256, A.desc, sorted, m, groups, gcount, plan, A.alloc);
+        launch(plan_add, persistent_grid(), 256, A.desc, sorted, grp, plan, A.alloc);
         launch(alloc_classes, 1, 64, A.alloc, status);
         unsigned long long *stats = with_stats ? status->counters : nullptr;
         const uint32_t *vals = forward ? d_av : d_au;
-        launch(mutate_add, persistent_grid(), 256, A.view(), A.desc, sorted, m, groups, gcount, plan, A.alloc,
-                                                          vals, big, bcount, stats, status);
-        launch(mutate_add_big, sms * 2, kTpbMut, A.view(), A.desc, sorted, m, groups, plan, A.alloc, vals, big,
-                                                        bcount, stats, status);
+        launch(mutate_add, persistent_grid(), 256, A.view(), A.desc, sorted, grp, plan, A.alloc, vals, big, bcount,
+               stats, status);
+        launch(mutate_add_big, sms * 2, kTpbMut, A.view(), A.desc, sorted, grp, plan, A.alloc, vals, big, bcount,
+               stats, status);
         prof_end(p);
         check_launch();
     }

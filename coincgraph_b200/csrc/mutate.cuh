@@ -97,39 +97,36 @@ __global__ void make_keys_add(const uint32_t *au, const uint32_t *av, uint32_t n
     }
 }
 
-// Group heads of a sorted key array (one group per source).
-__global__ void find_groups(const unsigned long long *keys, uint32_t m, uint32_t *groups, uint32_t *gcount) {
+// Source groups of a sorted key array, in key order: group g spans keys
+// [start[g], end[g]).  Built by group_flags, a device exclusive scan of the
+// flags and group_scatter, so a group's end is one load away.
+struct Groups {
+    const uint32_t *start;
+    const uint32_t *end;
+    const uint32_t *count;
+};
+
+__global__ void group_flags(const unsigned long long *keys, uint32_t m, uint32_t *flags) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    bool head = false;
-    if (i < m) {
-        const unsigned long long k = keys[i];
-        head = k != kKeyNone && (i == 0 || key_src(keys[i - 1]) != key_src(k));
-    }
-    if (__any_sync(kFull, i < m)) {
-        const uint32_t mask = __ballot_sync(kFull, head);
-        if (mask) {
-            const uint32_t leader = __ffs(mask) - 1;
-            uint32_t base = 0;
-            if (lane_id() == leader) base = atomicAdd(gcount, __popc(mask));
-            base = __shfl_sync(kFull, base, leader);
-            if (head) groups[base + __popc(mask & lanemask_lt())] = i;
-        }
-    }
+    if (i >= m) return;
+    const unsigned long long k = keys[i];
+    flags[i] = (k != kKeyNone && (i == 0 || key_src(keys[i - 1]) != key_src(k))) ? 1u : 0u;
 }
 
-// End of the group starting at `start`: first index whose source differs.
-__device__ __forceinline__ uint32_t group_end(const unsigned long long *keys, uint32_t m, uint32_t start) {
-    const uint32_t src = key_src(keys[start]);
-    uint32_t lo = start + 1, hi = m;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        const unsigned long long k = keys[mid];
-        if (k != kKeyNone && key_src(k) == src)
-            lo = mid + 1;
-        else
-            hi = mid;
+__global__ void group_scatter(const unsigned long long *keys, uint32_t m, const uint32_t *flags, const uint32_t *pos,
+                              uint32_t *start, uint32_t *end, uint32_t *count) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const unsigned long long k = keys[i];
+    if (k == kKeyNone) return;
+    if (flags[i]) {
+        start[pos[i]] = i;
+        if (pos[i] > 0) end[pos[i] - 1] = i;
     }
-    return lo;
+    if (i + 1 == m || keys[i + 1] == kKeyNone) {  // last valid key closes the last group
+        end[pos[i] + flags[i] - 1] = i + 1;
+        *count = pos[i] + flags[i];
+    }
 }
 
 // Deletion run of key `key` inside the group [gs, ge): the index of the
@@ -266,20 +263,21 @@ __device__ __forceinline__ uint32_t warp_tomb_global(const AdjView &view, const 
 // Deletion phase, one warp per source group; rows above kWarpRowMax go to
 // the block path.  Launched with kMutWarps * 32 threads per block.
 __global__ void __launch_bounds__(kMutWarps * 32)
-    mutate_delete(AdjView view, RowDesc *desc, const unsigned long long *keys, uint32_t m, const uint32_t *groups,
-                  const uint32_t *gcount, uint32_t *matched, uint32_t *big, uint32_t *big_count, uint32_t *compact,
-                  uint32_t *compact_count, unsigned long long *stats, Status *st) {
+    mutate_delete(AdjView view, RowDesc *desc, const unsigned long long *keys, Groups gr, const uint32_t *list,
+                  const uint32_t *list_count, uint32_t *matched, uint32_t *big, uint32_t *big_count,
+                  uint32_t *compact, uint32_t *compact_count, unsigned long long *stats, Status *st) {
     const uint32_t lane = lane_id();
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t ng = *gcount;
+    const uint32_t nl = *list_count;
     unsigned long long removed = 0, changed = 0;
-    for (uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ng; g += warps) {
-        const uint32_t gs = groups[g];
-        const uint32_t ge = group_end(keys, m, gs);
+    for (uint32_t li = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; li < nl; li += warps) {
+        const uint32_t g = list[li];
+        const uint32_t gs = gr.start[g];
+        const uint32_t ge = gr.end[g];
         const uint32_t u = key_src(keys[gs]);
         const RowDesc d = desc[u];
         if (d.len > kWarpRowMax) {
-            if (lane == 0) big[atomicAdd(big_count, 1u)] = gs;
+            if (lane == 0) big[atomicAdd(big_count, 1u)] = g;
             continue;
         }
         const uint32_t done = (ge - gs <= 32u) ? warp_tomb_regs(view, d, keys, gs, ge - gs)
@@ -309,7 +307,7 @@ constexpr uint32_t kFilterBits = 4096;
 __device__ __forceinline__ uint32_t filter_hash(uint32_t x) { return (x * 0x9E3779B1u) >> 20; }  // 12 bits
 
 __global__ void __launch_bounds__(kTpbMut)
-    mutate_delete_big(AdjView view, RowDesc *desc, const unsigned long long *keys, uint32_t m, const uint32_t *big,
+    mutate_delete_big(AdjView view, RowDesc *desc, const unsigned long long *keys, Groups gr, const uint32_t *big,
                       const uint32_t *big_count, uint32_t *matched, uint32_t *compact, uint32_t *compact_count,
                       unsigned long long *stats, Status *st) {
     __shared__ uint32_t skey[kBigKeys];
@@ -323,9 +321,9 @@ __global__ void __launch_bounds__(kTpbMut)
     __shared__ uint32_t left;
     const uint32_t tid = threadIdx.x;
     const uint32_t nb = *big_count;
-    for (uint32_t g = blockIdx.x; g < nb; g += gridDim.x) {
-        const uint32_t gs = big[g];
-        const uint32_t ge = group_end(keys, m, gs);
+    for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
+        const uint32_t gs = gr.start[big[b]];
+        const uint32_t ge = gr.end[big[b]];
         const uint32_t gm = ge - gs;
         const bool in_smem = gm <= kBigKeys;
         const uint32_t u = key_src(keys[gs]);
@@ -447,6 +445,173 @@ __global__ void __launch_bounds__(kTpbMut)
     }
 }
 
+// ---------------------------------------------------------------- flat deletion
+//
+// When no destination is requested twice for the same source in a batch
+// (every run has one key), the entry to tombstone for a key is simply the
+// first live occurrence, i.e. the minimum matching position, which an
+// atomicMin finds in any order.  Such rows are scanned in 512-entry warp
+// chunks spread evenly over the whole grid (a hub row no longer serialises
+// on one block); rows with repeated requests keep the position-ordered
+// kernels above.
+constexpr uint32_t kDelChunk = 512;
+constexpr uint32_t kSmemKeys = 256;
+
+// Classify groups: chunk count for flat rows, ordered list for the rest.
+// `chunks` must be zero beyond the group count (it is scanned whole).
+__global__ void del_classify(const RowDesc *desc, const unsigned long long *keys, Groups gr, uint32_t *chunks,
+                             uint32_t *ordered, uint32_t *ordered_count) {
+    const uint32_t ng = *gr.count;
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+        const uint32_t gs = gr.start[g];
+        const uint32_t ge = gr.end[g];
+        bool dup = false;
+        for (uint32_t i = gs; i + 1 < ge && !dup; ++i) dup = keys[i] == keys[i + 1];
+        if (dup) {
+            ordered[atomicAdd(ordered_count, 1u)] = g;
+            chunks[g] = 0;
+        } else {
+            chunks[g] = (desc[key_src(keys[gs])].len + kDelChunk - 1) / kDelChunk;
+        }
+    }
+}
+
+// Warps take contiguous ranges of 512-entry chunks (uniform work), find the
+// group of their first chunk by one binary search and then advance through
+// the groups in order; each chunk records the first live match of every key.
+// `chunk_end` is the inclusive prefix sum of `chunks` over scan_n entries.
+__global__ void __launch_bounds__(kMutWarps * 32)
+    del_scan(AdjView view, const RowDesc *desc, const unsigned long long *keys, Groups gr, const uint32_t *chunk_end,
+             uint32_t scan_n, uint32_t *firstpos) {
+    __shared__ uint32_t skeys[kMutWarps][kSmemKeys];
+    uint32_t *sk = skeys[threadIdx.x >> 5];
+    const uint32_t lane = lane_id();
+    const uint32_t ng = *gr.count;
+    const uint32_t total = scan_n ? chunk_end[scan_n - 1] : 0u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t per = (total + warps - 1) / warps;
+    const uint32_t c_begin = min(total, wid * per), c_end = min(total, c_begin + per);
+    uint32_t g = 0;
+    {
+        uint32_t lo = 0, hi = ng;  // first group whose inclusive end exceeds c_begin
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (chunk_end[mid] > c_begin)
+                hi = mid;
+            else
+                lo = mid + 1;
+        }
+        g = lo;
+    }
+    for (uint32_t c = c_begin; c < c_end; ++c) {
+        while (chunk_end[g] <= c) ++g;
+        const uint32_t k0 = (c - (g ? chunk_end[g - 1] : 0u)) * kDelChunk;
+        const uint32_t gs = gr.start[g];
+        const uint32_t ge = gr.end[g];
+        const uint32_t nk = ge - gs;
+        const uint32_t u = key_src(keys[gs]);
+        const RowDesc d = desc[u];
+        const unsigned long long uhi = static_cast<unsigned long long>(u) << kKeyShift;
+        const uint32_t kd = lane < nk ? key_low(keys[gs + lane]) : 0u;
+        if (nk > 32u && nk <= kSmemKeys) {
+            for (uint32_t j = lane; j < nk; j += 32u) sk[j] = key_low(keys[gs + j]);
+        }
+        __syncwarp();
+        // A 512-entry chunk never straddles a segment (segments hold 2^14).
+        const uint32_t *src = view.at(d.off + k0);
+#pragma unroll
+        for (uint32_t s = 0; s < kDelChunk / 128u; ++s) {
+            const uint32_t kk = k0 + 128u * s + 4u * lane;
+            uint32_t e[4] = {kTomb, kTomb, kTomb, kTomb};
+            if (kk < d.len) {
+                const uint4 q = *reinterpret_cast<const uint4 *>(src + 128u * s + 4u * lane);
+                e[0] = q.x;
+                e[1] = q.y;
+                e[2] = q.z;
+                e[3] = q.w;
+#pragma unroll
+                for (int t = 0; t < 4; ++t)
+                    if (kk + t >= d.len) e[t] = kTomb;
+            }
+            int hit[4] = {-1, -1, -1, -1};
+            if (nk <= 32u) {
+                for (uint32_t j = 0; j < nk; ++j) {
+                    const uint32_t kj = __shfl_sync(kFull, kd, j);
+#pragma unroll
+                    for (int t = 0; t < 4; ++t)
+                        if (e[t] == kj) hit[t] = static_cast<int>(j);
+                }
+            } else {
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    if (e[t] == kTomb) continue;
+                    if (nk <= kSmemKeys) {
+                        uint32_t a = 0, b = nk;
+                        while (a < b) {
+                            const uint32_t mid = (a + b) >> 1;
+                            if (sk[mid] < e[t])
+                                a = mid + 1;
+                            else
+                                b = mid;
+                        }
+                        if (a < nk && sk[a] == e[t]) hit[t] = static_cast<int>(a);
+                    } else {
+                        uint32_t run, req;
+                        if (find_run(keys, gs, ge, uhi | e[t], run, req)) hit[t] = static_cast<int>(run - gs);
+                    }
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+                if (hit[t] >= 0 && e[t] != kTomb) atomicMin(firstpos + gs + hit[t], kk + t);
+        }
+        __syncwarp();
+    }
+}
+
+// Tombstone the first match of every key found by del_scan.
+__global__ void del_apply(AdjView view, RowDesc *desc, const unsigned long long *keys, uint32_t m,
+                          const uint32_t *firstpos, unsigned long long *stats) {
+    uint32_t removed = 0;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t rounded = (m + 31u) & ~31u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rounded; i += stride) {
+        if (i < m) {
+            const uint32_t p = firstpos[i];
+            if (p != kInf) {
+                const uint32_t u = key_src(keys[i]);
+                write_slot(view, desc[u].off + p, kTomb);
+                atomicAdd(&desc[u].meta, 1u << 6);
+                ++removed;
+            }
+        }
+    }
+    if (stats) warp_count(&stats[kCntRemoved], removed);
+}
+
+// Queue flat rows whose tombstones reached a quarter of their length.
+__global__ void del_finish(const RowDesc *desc, const unsigned long long *keys, Groups gr, const uint32_t *chunks,
+                           const uint32_t *firstpos, uint32_t *compact, uint32_t *compact_count,
+                           unsigned long long *stats) {
+    const uint32_t ng = *gr.count;
+    unsigned long long changed = 0;
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+        if (!chunks[g]) continue;  // ordered group, or empty row
+        const uint32_t gs = gr.start[g];
+        const uint32_t ge = gr.end[g];
+        bool any = false;
+        for (uint32_t i = gs; i < ge && !any; ++i) any = firstpos[i] != kInf;
+        if (!any) continue;
+        ++changed;
+        const uint32_t u = key_src(keys[gs]);
+        const RowDesc d = desc[u];
+        const uint32_t tombs = rd_tombs(d);
+        if (4ull * tombs >= d.len || tombs >= kMaxTombs / 2) compact[atomicAdd(compact_count, 1u)] = u;
+    }
+    if (stats && changed) atomicAdd(&stats[kCntChanged], changed);
+}
+
 // ---------------------------------------------------------------- compaction
 
 // Drop the tombstones of the queued rows in place (order kept).  One block
@@ -504,12 +669,12 @@ __global__ void __launch_bounds__(kTpbMut) compact_rows(AdjView view, RowDesc *d
 // Addition plan: rows that outgrow their block get a class (sized for the
 // live entries plus the additions, since relocation drops tombstones) and a
 // rank in that class.
-__global__ void plan_add(const RowDesc *desc, const unsigned long long *keys, uint32_t m, const uint32_t *groups,
-                         const uint32_t *gcount, unsigned long long *plan, ArenaAlloc *al) {
-    const uint32_t ng = *gcount;
+__global__ void plan_add(const RowDesc *desc, const unsigned long long *keys, Groups gr, unsigned long long *plan,
+                         ArenaAlloc *al) {
+    const uint32_t ng = *gr.count;
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
-        const uint32_t gs = groups[g];
-        const uint32_t ge = group_end(keys, m, gs);
+        const uint32_t gs = gr.start[g];
+        const uint32_t ge = gr.end[g];
         const RowDesc d = desc[key_src(keys[gs])];
         const unsigned long long used = static_cast<unsigned long long>(d.len) + (ge - gs);
         const unsigned long long live = static_cast<unsigned long long>(rd_live(d)) + (ge - gs);
@@ -568,14 +733,13 @@ __global__ void alloc_classes(ArenaAlloc *al, Status *st) {
 // Addition phase, one warp per group (rows above kWarpRowMax that must move
 // go to the block path).  `vals` is add_v for the forward arena and add_u
 // for the reverse arena.  A moving row is copied without its tombstones.
-__global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long *keys, uint32_t m,
-                           const uint32_t *groups, const uint32_t *gcount, const unsigned long long *plan,
-                           const ArenaAlloc *al, const uint32_t *vals, uint32_t *big, uint32_t *big_count,
-                           unsigned long long *stats, Status *st) {
+__global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long *keys, Groups gr,
+                           const unsigned long long *plan, const ArenaAlloc *al, const uint32_t *vals, uint32_t *big,
+                           uint32_t *big_count, unsigned long long *stats, Status *st) {
     if (ld_volatile(&st->err) & kErrArena) return;
     const uint32_t lane = lane_id();
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t ng = *gcount;
+    const uint32_t ng = *gr.count;
     unsigned long long changed = 0, moved = 0;
     for (uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ng; g += warps) {
         const unsigned long long p = plan[g];
@@ -583,8 +747,8 @@ __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long
             if (lane == 0) set_error(st, kErrInternal, g);
             continue;
         }
-        const uint32_t gs = groups[g];
-        const uint32_t ge = group_end(keys, m, gs);
+        const uint32_t gs = gr.start[g];
+        const uint32_t ge = gr.end[g];
         const uint32_t u = key_src(keys[gs]);
         const RowDesc d = desc[u];
         const uint32_t a = ge - gs;
@@ -619,7 +783,7 @@ __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long
 }
 
 __global__ void __launch_bounds__(kTpbMut)
-    mutate_add_big(AdjView view, RowDesc *desc, const unsigned long long *keys, uint32_t m, const uint32_t *groups,
+    mutate_add_big(AdjView view, RowDesc *desc, const unsigned long long *keys, Groups gr,
                    const unsigned long long *plan, const ArenaAlloc *al, const uint32_t *vals, const uint32_t *big,
                    const uint32_t *big_count, unsigned long long *stats, Status *st) {
     using BlockScan = cub::BlockScan<uint32_t, kTpbMut>;
@@ -629,8 +793,8 @@ __global__ void __launch_bounds__(kTpbMut)
     for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
         const uint32_t g = big[b];
         const unsigned long long p = plan[g];
-        const uint32_t gs = groups[g];
-        const uint32_t ge = group_end(keys, m, gs);
+        const uint32_t gs = gr.start[g];
+        const uint32_t ge = gr.end[g];
         const uint32_t u = key_src(keys[gs]);
         const RowDesc d = desc[u];
         const uint32_t a = ge - gs;
