@@ -54,7 +54,7 @@ def build_engine(force: bool = False, verbose_ptxas: bool = False) -> str:
     if force or verbose_ptxas or _stale(out, deps):
         cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
                "-Xcompiler", "-fPIC", "-shared", "-I" + INCLUDE,
-               os.path.join(CSRC, "engine.cu"), "-o", out]
+               os.path.join(CSRC, "engine.cu"), os.path.join(CSRC, "noalloc.cu"), "-o", out]
         if verbose_ptxas:
             cmd.insert(1, "-Xptxas=-v")
         log = _run(cmd)

@@ -1179,6 +1179,12 @@ struct cig_handle {
 
 namespace {
 thread_local std::string g_create_error;
+}  // namespace
+
+// Error message of a failed call that has no handle (read by cig_last_error(NULL)).
+void cig_set_unbound_error(const std::string &message) { g_create_error = message; }
+
+namespace {
 
 template <class F>
 int guarded(cig_handle *h, F f) {

@@ -132,6 +132,7 @@ SIGNATURES = [
     ("cig_graph_info_get", _i32, [_vp, ctypes.POINTER(GraphInfo)]),
     ("cig_profile_enable", _i32, [_vp, _i32]),
     ("cig_profile_read", _i32, [_vp, ctypes.POINTER(StageProfile), _u32]),
+    ("cig_bfs_csr_noalloc", _i32, [_vp, _vp, _u32, _u32, _vp, _vp]),
     ("cig_query_bfs_multi", _i32, [_vp, _vp, _u32, _vp]),
     ("cig_query_sssp_multi", _i32, [_vp, _vp, _u32, _vp]),
     ("cig_version", ctypes.c_char_p, []),

@@ -202,6 +202,27 @@ typedef struct {
 int cig_profile_enable(cig_handle *h, int enable);
 int cig_profile_read(cig_handle *h, cig_stage_profile *out, uint32_t count);
 
+/* BFS depths over a CSR already in device memory, with no device
+ * allocation.  No counterpart in the reference.  For callers that cannot
+ * allocate at the point of use: code running during CUDA stream capture
+ * (cudaMalloc cannot be captured), serving loops that must avoid
+ * cudaMalloc/cudaFree and their implicit device synchronisation, and hosts
+ * whose device memory pool belongs to someone else.
+ *   xadj[n+1] (uint64) and adj[xadj[n]] (uint32): device CSR, rows in any order;
+ *   depth[n] (uint32): device output, 0xFFFFFFFF for unreached vertices;
+ *   stream: a cudaStream_t (NULL = the legacy default stream); the call
+ *   returns after the work on that stream has finished.
+ * All scratch lives in a fixed __device__ array sized for at most
+ * CIG_NOALLOC_MAX_VERTICES vertices (about 3 MiB held by every GPU that loads
+ * the library); larger n is rejected with CIG_ERR_ARG.  The first call on a
+ * device looks up that array's device address, so make the first call on
+ * each device before any stream capture.  Calls on one device share the
+ * array: calls that overlap on the GPU race and must be serialised.
+ * Errors: the message is available from cig_last_error(NULL). */
+#define CIG_NOALLOC_MAX_VERTICES (1u << 18)
+int cig_bfs_csr_noalloc(const uint64_t *xadj, const uint32_t *adj, uint32_t n, uint32_t source, uint32_t *depth,
+                        void *stream);
+
 /* Library version string. */
 const char *cig_version(void);
 
