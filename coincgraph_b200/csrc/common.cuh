@@ -110,6 +110,7 @@ enum Counter : int {
     kCntSegEvicted = 11,
     kCntPrRounds = 12,
     kCntRemoved = 13,
+    kCntSrcEdges = 14,  // multi-source queries: sum of (source bits x row length) over expanded rows
     // Per-kernel groups of 4: edges, edges from HBM, rows expanded, hits.
     kCntPush = 16,
     kCntInval = 20,

@@ -29,6 +29,7 @@
 #include "expand.cuh"
 #include "mutate.cuh"
 #include "pr.cuh"
+#include "query.cuh"
 #include "traverse.cuh"
 
 using namespace cig;
@@ -372,6 +373,14 @@ struct cig_handle {
         ++n_launch;
     }
 
+    template <class... P>
+    void launch_coop_on(cudaStream_t st, void (*kernel)(P...), int tpb, typename Identity<P>::type... args) {
+        void *argv[] = {static_cast<void *>(&args)...};
+        const int blocks = coop_blocks(kernel, tpb);
+        CK(cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(kernel), dim3(blocks), dim3(tpb), argv, 0, st));
+        ++n_launch;
+    }
+
     void check_launch() { CK(cudaGetLastError()); }
 
     uint64_t launch_mark = 0;
@@ -480,6 +489,7 @@ struct cig_handle {
         dfree(pr_queued);
         free_batch();
         dfree(tmp_u32);
+        free_queries();
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -643,12 +653,16 @@ struct cig_handle {
         } else {
             budget_slots = opt.cache_gib > 0 ? static_cast<uint64_t>(opt.cache_gib * 1073741824.0 / 4.0) : 0;
         }
+        // Slots left over after the used segments go to the headroom segments
+        // that the block allocator hands out later, so relocated rows land in
+        // HBM while the budget lasts.
         cache_slots = std::min<uint64_t>(budget_slots >> kSegShift, fwd.seg_total);
-        resident = std::min<uint64_t>(cache_slots, fwd.seg_used);
+        resident = cache_slots;
         if (cache_slots) {
             dmalloc(fwd.dev, cache_slots * kSegEdges);
-            if (resident)
-                CK(cudaMemcpy(fwd.dev, fwd.host, resident * kSegEdges * sizeof(uint32_t), cudaMemcpyHostToDevice));
+            const uint64_t filled = std::min<uint64_t>(cache_slots, fwd.seg_used);
+            if (filled)
+                CK(cudaMemcpy(fwd.dev, fwd.host, filled * kSegEdges * sizeof(uint32_t), cudaMemcpyHostToDevice));
         }
         {
             std::vector<int32_t> slot(fwd.seg_total, -1);
@@ -1155,6 +1169,146 @@ struct cig_handle {
         return h;
     }
 
+    // ------------------------------------------------------------ multi-source queries
+    // Queries run on their own stream with their own status word and buffers,
+    // ordered after the updates already issued on the engine stream.  They
+    // read the forward rows (cache or zero-copy) and change no engine state.
+    cudaStream_t qstream = nullptr;
+    Status *qstatus = nullptr;
+    Status *h_qstatus = nullptr;
+    cudaEvent_t q_ev[3] = {};
+    uint32_t *ms_dist = nullptr;
+    unsigned long long *ms_visit = nullptr, *ms_mask0 = nullptr, *ms_mask1 = nullptr;
+    uint32_t *ms_q0 = nullptr, *ms_q1 = nullptr, *ms_small = nullptr, *ms_src = nullptr, *ms_out = nullptr;
+    uint64_t ms_out_cap = 0;
+    BigRow *ms_big = nullptr;
+
+    void alloc_queries() {
+        if (qstream) return;
+        CK(cudaStreamCreateWithFlags(&qstream, cudaStreamNonBlocking));
+        for (auto &e : q_ev) CK(cudaEventCreate(&e));
+        dmalloc(qstatus, 1);
+        CK(cudaHostAlloc(reinterpret_cast<void **>(&h_qstatus), sizeof(Status), cudaHostAllocDefault));
+        dmalloc(ms_dist, static_cast<size_t>(n) * kMsWidth);
+        dmalloc(ms_visit, n);
+        dmalloc(ms_mask0, n);
+        dmalloc(ms_mask1, n);
+        dmalloc(ms_q0, n + 1);
+        dmalloc(ms_q1, n + 1);
+        dmalloc(ms_small, 8);
+        dmalloc(ms_src, kMsWidth);
+        dmalloc(ms_big, kBigRowCap);
+    }
+
+    void free_queries() {
+        if (qstream) cudaStreamSynchronize(qstream);
+        for (auto &e : q_ev)
+            if (e) cudaEventDestroy(e);
+        dfree(qstatus);
+        if (h_qstatus) cudaFreeHost(h_qstatus);
+        h_qstatus = nullptr;
+        dfree(ms_dist);
+        dfree(ms_visit);
+        dfree(ms_mask0);
+        dfree(ms_mask1);
+        dfree(ms_q0);
+        dfree(ms_q1);
+        dfree(ms_small);
+        dfree(ms_src);
+        dfree(ms_big);
+        dfree(ms_out);
+        if (qstream) cudaStreamDestroy(qstream);
+        qstream = nullptr;
+    }
+
+    // k sources in waves of `width` (1..64) sources; results k x n source-major
+    // in device memory `out`.  width 64 is the batched form, width 1 the plain
+    // per-source form over the same kernels.
+    void query_multi(int algo, const uint32_t *sources, uint32_t k, uint32_t width, uint32_t *out,
+                     cig_query_stats *qs) {
+        if (!loaded) throw CigError(CIG_ERR_ARG, "load a graph first");
+        require_alive();
+        if (algo != CIG_BFS && algo != CIG_SSSP) throw CigError(CIG_ERR_ARG, "queries are BFS or SSSP");
+        if (!sources || !out) throw CigError(CIG_ERR_ARG, "null sources or output");
+        if (width == 0 || width > kMsWidth) throw CigError(CIG_ERR_ARG, "wave width must be 1..64");
+        for (uint32_t j = 0; j < k; ++j)
+            if (sources[j] >= n) throw CigError(CIG_ERR_ARG, "query source out of range");
+        alloc_queries();
+        CK(cudaMemsetAsync(qstatus, 0, sizeof(Status), qstream));
+        CK(cudaEventRecord(q_ev[0], stream));
+        CK(cudaStreamWaitEvent(qstream, q_ev[0], 0));
+        CK(cudaEventRecord(q_ev[1], qstream));
+        const uint64_t launches0 = n_launch;
+        uint32_t waves = 0;
+        for (uint32_t j0 = 0; j0 < k; j0 += width, ++waves) {
+            const uint32_t kw = std::min(width, k - j0);
+            CK(cudaMemsetAsync(ms_dist, 0xFF, static_cast<size_t>(n) * width * sizeof(uint32_t), qstream));
+            CK(cudaMemsetAsync(ms_mask0, 0, n * sizeof(unsigned long long), qstream));
+            CK(cudaMemsetAsync(ms_mask1, 0, n * sizeof(unsigned long long), qstream));
+            if (algo == CIG_BFS)
+                CK(cudaMemsetAsync(ms_visit, 0, n * sizeof(unsigned long long), qstream));
+            CK(cudaMemsetAsync(ms_small, 0, 8 * sizeof(uint32_t), qstream));
+            CK(cudaMemcpyAsync(ms_src, sources + j0, kw * sizeof(uint32_t), cudaMemcpyHostToDevice, qstream));
+            const MsFrontier fr{ms_q0, ms_q1, ms_small, ms_mask0, ms_mask1, n + 1};
+            const BigList bl{ms_big, ms_small + 3, kBigRowCap};
+            ms_seed<<<1, kMsWidth, 0, qstream>>>(ms_src, kw, ms_dist, width, algo == CIG_BFS ? ms_visit : nullptr,
+                                                 fr, qstatus);
+            ++n_launch;
+            if (algo == CIG_BFS)
+                launch_coop_on(qstream, ms_closure<kBfs>, kTpbMs, fwd.view(), ms_dist, width, ms_visit, fr, bl, n + 2,
+                               qstatus);
+            else
+                launch_coop_on(qstream, ms_closure<kSssp>, kTpbMs, fwd.view(), ms_dist, width,
+                               static_cast<unsigned long long *>(nullptr), fr, bl, n + 2, qstatus);
+            ms_transpose<<<(n + kMsTile - 1) / kMsTile, 256, 0, qstream>>>(ms_dist, n, width, kw,
+                                                                         out + static_cast<uint64_t>(j0) * n);
+            ++n_launch;
+            check_launch();
+        }
+        CK(cudaEventRecord(q_ev[2], qstream));
+        CK(cudaStreamSynchronize(qstream));
+        CK(cudaMemcpy(h_qstatus, qstatus, sizeof(Status), cudaMemcpyDeviceToHost));
+        if (h_qstatus->err) {
+            std::string what;
+            if (h_qstatus->err & kErrRounds) what += "round bound exceeded; ";
+            if (h_qstatus->err & kErrBarrier) what += "grid barrier wait limit exceeded; ";
+            if (h_qstatus->err & kErrQueue) what += "work queue overflow; ";
+            throw CigError(CIG_ERR_LIMIT, "query: device reported: " + what + "info=" +
+                                              std::to_string(h_qstatus->err_info));
+        }
+        if (qs) {
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, q_ev[1], q_ev[2]));
+            std::memset(qs, 0, sizeof(*qs));
+            qs->ms = ms;
+            qs->edges_scanned = h_qstatus->counters[kCntPush + 0];
+            qs->edges_scanned_cached = h_qstatus->counters[kCntPush + 1];
+            qs->rows_expanded = h_qstatus->counters[kCntPush + 2];
+            qs->source_edges = h_qstatus->counters[kCntSrcEdges];
+            qs->rounds = h_qstatus->counters[kCntRounds];
+            qs->waves = waves;
+            qs->kernel_launches = n_launch - launches0;
+        }
+    }
+
+    // Host-output form: k x n values copied to host memory `out`.
+    void query_multi_host(int algo, const uint32_t *sources, uint32_t k, uint32_t *out) {
+        if (!out) throw CigError(CIG_ERR_ARG, "null output");
+        if (!loaded) throw CigError(CIG_ERR_ARG, "load a graph first");
+        const uint64_t need = static_cast<uint64_t>(std::min<uint32_t>(k, kMsWidth)) * n;
+        if (need > ms_out_cap) {
+            dfree(ms_out);
+            dmalloc(ms_out, need);
+            ms_out_cap = need;
+        }
+        for (uint32_t j0 = 0; j0 < k; j0 += kMsWidth) {
+            const uint32_t kw = std::min(kMsWidth, k - j0);
+            query_multi(algo, sources + j0, kw, kMsWidth, ms_out, nullptr);
+            CK(cudaMemcpy(out + static_cast<uint64_t>(j0) * n, ms_out, static_cast<uint64_t>(kw) * n * sizeof(uint32_t),
+                          cudaMemcpyDeviceToHost));
+        }
+    }
+
     // Make the pinned host arena current (write back dirty cache segments).
     void flush_host() {
         if (!loaded) throw CigError(CIG_ERR_ARG, "load a graph first");
@@ -1398,7 +1552,7 @@ int cig_graph_info_get(cig_handle *h, cig_graph_info *info) {
         info->arena_used_edges = std::min<uint64_t>(al.seg_bump, h->fwd.seg_total) * kSegEdges;
         info->segment_edges = kSegEdges;
         info->segments_total = h->fwd.seg_total;
-        info->segments_resident = h->resident;
+        info->segments_resident = std::min<uint64_t>(h->resident, std::min<uint64_t>(al.seg_bump, h->fwd.seg_total));
         info->cache_capacity_segments = h->cache_slots;
         size_t free_b = 0, total_b = 0;
         cudaMemGetInfo(&free_b, &total_b);
@@ -1424,14 +1578,17 @@ int cig_profile_read(cig_handle *h, cig_stage_profile *out, uint32_t count) {
     });
 }
 
-int cig_query_bfs_multi(cig_handle *h, const uint32_t *, uint32_t, uint32_t *) {
-    if (h) h->err = "multi-source queries are not built yet";
-    return CIG_ERR_NOTIMPL;
+int cig_query_bfs_multi(cig_handle *h, const uint32_t *sources, uint32_t k, uint32_t *out_depth) {
+    return guarded(h, [&] { h->query_multi_host(CIG_BFS, sources, k, out_depth); });
 }
 
-int cig_query_sssp_multi(cig_handle *h, const uint32_t *, uint32_t, uint32_t *) {
-    if (h) h->err = "multi-source queries are not built yet";
-    return CIG_ERR_NOTIMPL;
+int cig_query_sssp_multi(cig_handle *h, const uint32_t *sources, uint32_t k, uint32_t *out_dist) {
+    return guarded(h, [&] { h->query_multi_host(CIG_SSSP, sources, k, out_dist); });
+}
+
+int cig_query_multi_device(cig_handle *h, int algo, const uint32_t *sources, uint32_t k, uint32_t width,
+                           uint32_t *out_device, cig_query_stats *stats) {
+    return guarded(h, [&] { h->query_multi(algo, sources, k, width, out_device, stats); });
 }
 
 const char *cig_version(void) { return kVersion; }

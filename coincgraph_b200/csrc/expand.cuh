@@ -19,14 +19,17 @@
 
 namespace cig {
 
-template <int TPB>
+// P is the per-row payload handed to Op::edge: a 32-bit value for the
+// maintained algorithms, a 64-bit source mask for multi-source queries.
+template <int TPB, class P = uint32_t>
 struct ExpandSmem {
     uint32_t owner;
-    uint32_t b_x, b_payload, b_deg;
+    uint32_t b_x, b_deg;
+    P b_payload;
     unsigned long long b_off;
     uint32_t f_scan[TPB];
     uint32_t f_x[TPB];
-    uint32_t f_payload[TPB];
+    P f_payload[TPB];
     const uint32_t *f_ptr[TPB];
 };
 
@@ -58,7 +61,8 @@ constexpr uint32_t kSplitChunk = 1024;
 
 struct BigRow {
     unsigned long long off;
-    uint32_t x, payload, deg, pad;
+    unsigned long long payload;
+    uint32_t x, deg;
 };
 
 struct Defer {
@@ -67,12 +71,12 @@ struct Defer {
     uint32_t cap;
 };
 
-// Op must provide: __device__ bool edge(bool valid, uint32_t x, uint32_t payload, uint32_t y) const;
+// Op must provide: __device__ bool edge(bool valid, uint32_t x, P payload, uint32_t y) const;
 // returning true when the edge changed state.
 // edge() is called by all 32 lanes of a warp together (valid=false on padding lanes).
-template <int TPB, class Op>
-__device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint32_t x, uint32_t payload,
-                                            uint64_t off, uint32_t deg, const Op &op, ExpandSmem<TPB> &sm,
+template <int TPB, class Op, class P>
+__device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint32_t x, P payload,
+                                            uint64_t off, uint32_t deg, const Op &op, ExpandSmem<TPB, P> &sm,
                                             ExpandCounters &cnt, const Defer &defer = Defer{nullptr, nullptr, 0}) {
     const uint32_t lane = lane_id();
     const uint32_t warp = threadIdx.x >> 5;
@@ -84,7 +88,7 @@ __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint3
     if (has && defer.rows && deg >= kSplitDeg) {
         const uint32_t i = atomicAdd(defer.count, 1u);
         if (i < defer.cap) {
-            defer.rows[i] = BigRow{off, x, payload, deg, 0u};
+            defer.rows[i] = BigRow{off, static_cast<unsigned long long>(payload), x, deg};
             has = false;
         }
     }
@@ -103,7 +107,8 @@ __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint3
             big = false;
         }
         __syncthreads();
-        const uint32_t bx = sm.b_x, bp = sm.b_payload, bdeg = sm.b_deg;
+        const uint32_t bx = sm.b_x, bdeg = sm.b_deg;
+        const P bp = sm.b_payload;
         const uint64_t boff = sm.b_off;
         if (bdeg <= kSegEdges) {
             const uint32_t *rp = view.at(boff);
@@ -130,7 +135,7 @@ __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint3
     while ((mmask = __ballot_sync(kFull, med)) != 0u) {
         const uint32_t leader = __ffs(mmask) - 1;
         const uint32_t wx = __shfl_sync(kFull, x, leader);
-        const uint32_t wp = __shfl_sync(kFull, payload, leader);
+        const P wp = __shfl_sync(kFull, payload, leader);
         const uint32_t wdeg = __shfl_sync(kFull, deg, leader);
         const uint64_t woff = __shfl_sync(kFull, static_cast<unsigned long long>(off), leader);
         if (lane == leader) med = false;
@@ -162,7 +167,8 @@ __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint3
     for (uint32_t base = 0; base < total; base += 32u) {
         const uint32_t e = base + lane;
         const bool valid = e < total;
-        uint32_t ox = 0, op_ = 0, y = 0;
+        uint32_t ox = 0, y = 0;
+        P op_ = 0;
         if (valid) {
             // Last lane whose exclusive prefix is <= e owns edge e.
             uint32_t lo = 0, hi = 32;
@@ -185,7 +191,7 @@ __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint3
 // Expand the deferred rows: chunk g of the concatenated chunk sequence goes
 // to block g mod gridDim.x.  Every block walks the (short) list in the same
 // order, so the assignment needs no coordination.  Block-uniform loops.
-template <int TPB, class Op>
+template <int TPB, class P = uint32_t, class Op>
 __device__ __forceinline__ void expand_deferred(const AdjView &view, const BigRow *rows, uint32_t nrows,
                                                 const Op &op, ExpandCounters &cnt) {
     const uint32_t grid = gridDim.x;
@@ -200,7 +206,7 @@ __device__ __forceinline__ void expand_deferred(const AdjView &view, const BigRo
                 const uint32_t k = base + kk + threadIdx.x;
                 const bool valid = k < r.deg;
                 const uint32_t y = valid ? __ldg(view.at(r.off + k)) : 0u;
-                cnt.hits += op.edge(valid && y != kTomb, r.x, r.payload, y);
+                cnt.hits += op.edge(valid && y != kTomb, r.x, static_cast<P>(r.payload), y);
             }
         }
         prefix += chunks;

@@ -88,6 +88,22 @@ class GraphInfo(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class QueryStats(ctypes.Structure):
+    _fields_ = [
+        ("ms", ctypes.c_double),
+        ("edges_scanned", ctypes.c_uint64),
+        ("edges_scanned_cached", ctypes.c_uint64),
+        ("rows_expanded", ctypes.c_uint64),
+        ("source_edges", ctypes.c_uint64),
+        ("rounds", ctypes.c_uint64),
+        ("waves", ctypes.c_uint64),
+        ("kernel_launches", ctypes.c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 STAGES = ["group", "mutate", "seed", "inval", "pull", "push", "pr", "cache", "mutate_rev", "add", "add_rev"]
 
 
@@ -135,6 +151,7 @@ SIGNATURES = [
     ("cig_bfs_csr_noalloc", _i32, [_vp, _vp, _u32, _u32, _vp, _vp]),
     ("cig_query_bfs_multi", _i32, [_vp, _vp, _u32, _vp]),
     ("cig_query_sssp_multi", _i32, [_vp, _vp, _u32, _vp]),
+    ("cig_query_multi_device", _i32, [_vp, _i32, _vp, _u32, _u32, _vp, ctypes.POINTER(QueryStats)]),
     ("cig_version", ctypes.c_char_p, []),
 ]
 
@@ -296,6 +313,30 @@ class Engine:
             s = np.empty(self.n, dtype=np.float32)
             self._check(self.lib.cig_get_pr(self.h, _ptr(r), _ptr(s)))
         return r, s
+
+    # -- multi-source queries on the current graph
+    def query_bfs(self, sources) -> np.ndarray:
+        """k x n BFS depths (UINT32_MAX for unreached), k = len(sources)."""
+        src = _u32arr(sources)
+        out = np.empty((len(src), self.n), dtype=np.uint32)
+        self._check(self.lib.cig_query_bfs_multi(self.h, _ptr(src), len(src), _ptr(out)))
+        return out
+
+    def query_sssp(self, sources) -> np.ndarray:
+        """k x n SSSP distances (UINT32_MAX for unreached), k = len(sources)."""
+        src = _u32arr(sources)
+        out = np.empty((len(src), self.n), dtype=np.uint32)
+        self._check(self.lib.cig_query_sssp_multi(self.h, _ptr(src), len(src), _ptr(out)))
+        return out
+
+    def query_device(self, algo: str, sources, out, width: int = 64) -> dict:
+        """Results into device memory `out` (k x n words, e.g. a torch CUDA
+        tensor); width 64 = batched bitmask waves, 1 = per-source form."""
+        src = _u32arr(sources)
+        s = QueryStats()
+        self._check(self.lib.cig_query_multi_device(self.h, ALGOS[algo], _ptr(src), len(src), width, _ptr(out),
+                                                    ctypes.byref(s)))
+        return s.as_dict()
 
     def digest(self) -> int:
         out = ctypes.c_uint64()

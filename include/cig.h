@@ -170,6 +170,26 @@ int cig_graph_info_get(cig_handle *h, cig_graph_info *info);
 int cig_query_bfs_multi(cig_handle *h, const uint32_t *sources, uint32_t k, uint32_t *out_depth);
 int cig_query_sssp_multi(cig_handle *h, const uint32_t *sources, uint32_t k, uint32_t *out_dist);
 
+typedef struct {
+    double ms;                     /* device time of the whole query (all waves) */
+    uint64_t edges_scanned;        /* adjacency entries read: edge-scans, the GTEPS numerator */
+    uint64_t edges_scanned_cached; /* of which from HBM */
+    uint64_t rows_expanded;
+    uint64_t source_edges;         /* sum over expanded rows of (source bits x row length) */
+    uint64_t rounds;
+    uint64_t waves;
+    uint64_t kernel_launches;
+} cig_query_stats;
+
+/* Device-memory form of the two calls above for callers that keep results
+ * on the GPU: `algo` is CIG_BFS or CIG_SSSP, `sources` a host array of k
+ * vertex ids, `out_device` a device array of k x n words.  Sources run in
+ * waves of `width` (1..64): 64 is the batched bitmask form, 1 the plain
+ * per-source form over the same kernels.  No reference counterpart (the
+ * reference runs one source per engine run). */
+int cig_query_multi_device(cig_handle *h, int algo, const uint32_t *sources, uint32_t k, uint32_t width,
+                           uint32_t *out_device, cig_query_stats *stats);
+
 /* Per-stage device time and work counters, measured with CUDA events on the
  * engine's own stream.  Replaces the reference's [ATTR] stage attribution
  * (samples/hybrid_sssp/hybrid_sssp.cu:496-512) and its NVTX marks

@@ -58,3 +58,4 @@ def test_struct_layouts(built):
     assert ctypes.sizeof(engine.Options) == 48
     assert ctypes.sizeof(engine.BatchStats) == 20 * 8
     assert ctypes.sizeof(engine.StageProfile) == 6 * 8
+    assert ctypes.sizeof(engine.QueryStats) == 8 * 8
