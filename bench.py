@@ -56,9 +56,16 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--ref-budget-s", type=float, default=150.0,
                    help="reference arm: stop timing after this much CPU time")
-    p.add_argument("--workload", default="stream", choices=["stream", "msbfs", "mssssp"],
+    p.add_argument("--workload", default="stream",
+                   choices=["stream", "msbfs", "mssssp", "uneven", "served", "pr"],
                    help="stream: the update-stream benchmark (default); msbfs/mssssp: 64-source queries "
-                        "on a symmetric R-MAT graph, batched bitmask waves vs the per-source form")
+                        "on a symmetric R-MAT graph, batched bitmask waves vs the per-source form; uneven: "
+                        "batches of log-uniform sizes, batched form (one sync) vs one call per batch")
+    p.add_argument("--requests", type=int, default=400, help="served: requests in the stream")
+    p.add_argument("--update-frac", type=float, default=0.1, help="served: share of update requests")
+    p.add_argument("--rate", type=float, default=0.0, help="served: Poisson arrival rate, requests/s (0: all at once)")
+    p.add_argument("--uneven-batches", type=int, default=20)
+    p.add_argument("--uneven-max", type=int, default=1_000_000)
     p.add_argument("--sources", type=int, default=64)
     return p.parse_args()
 
@@ -165,9 +172,19 @@ def link_peak_gbs(torch, dev):
 ROW_BYTES, EDGE_STATE_BYTES, ADJ_BYTES, HIT_BYTES = 28, 8, 4, 16
 
 
-def stage_roofline(prof_stage, hbm_peak, link_peak):
+# Flat deletion scan: per row entry read a 4-byte adjacency word (HBM when
+# its segment is resident, else the host link); per deletion key an 8-byte
+# key read and a 4-byte first-match word.
+DEL_KEY_BYTES = 12
+
+
+def stage_roofline(prof_stage, hbm_peak, link_peak, kind="traversal"):
     edges, cached = prof_stage["edges"], prof_stage["edges_cached"]
-    hbm = prof_stage["rows"] * ROW_BYTES + edges * EDGE_STATE_BYTES + cached * ADJ_BYTES + prof_stage["hits"] * HIT_BYTES
+    if kind == "del_scan":
+        hbm = cached * ADJ_BYTES + prof_stage["hits"] * DEL_KEY_BYTES
+    else:
+        hbm = (prof_stage["rows"] * ROW_BYTES + edges * EDGE_STATE_BYTES + cached * ADJ_BYTES
+               + prof_stage["hits"] * HIT_BYTES)
     link = (edges - cached) * ADJ_BYTES
     t = prof_stage["ms"] * 1e-3
     if t <= 0:
@@ -175,6 +192,23 @@ def stage_roofline(prof_stage, hbm_peak, link_peak):
     t_roof = hbm / (hbm_peak * 1e9) + link / (link_peak * 1e9)
     return {"hbm_bytes": hbm, "link_bytes": link, "seconds": t, "achieved_hbm_gbs": hbm / t / 1e9,
             "achieved_link_gbs": link / t / 1e9, "t_roof_s": t_roof, "frac_combined": t_roof / t}
+
+
+def traffic_ratio(kernel):
+    """DRAM bytes per algorithmic HBM byte of `kernel` from profiles/traffic.md
+    (an ncu capture of a smaller case of the same kernel), or None."""
+    path = os.path.join(ROOT, "profiles", "traffic.md")
+    if not os.path.exists(path):
+        return None, None
+    with open(path) as f:
+        for line in f:
+            cells = [c.strip() for c in line.strip().strip("|").split("|")]
+            if len(cells) == 5 and cells[0] == kernel:
+                try:
+                    return float(cells[4]), cells[1]
+                except ValueError:
+                    return None, None
+    return None, None
 
 
 def cpu_baseline(g, ups, args, batch_index):
@@ -350,24 +384,39 @@ def run_ours(args):
     hbm_peak, peak_kind = load_peaks()
     link_peak = link_peak_gbs(torch, dev)
     stages = {}
-    for name in ("group", "mutate", "mutate_rev", "add", "add_rev", "seed", "inval", "pull", "push"):
+    for name in ("group", "mutate", "mutate_rev", "add", "add_rev", "seed", "inval", "pull", "push", "del_scan"):
         stages[name] = {"ms_per_batch": prof[name]["ms"] / args.steps, "launches": prof[name]["launches"]}
-    trav = {n: stage_roofline(prof[n], hbm_peak, link_peak) for n in ("inval", "pull", "push")}
-    dominant = max(("push", "inval", "pull"), key=lambda n: prof[n]["ms"])
-    rf = trav[dominant]
+    kern = {n: stage_roofline(prof[n], hbm_peak, link_peak, "del_scan" if n == "del_scan" else "traversal")
+            for n in ("del_scan", "inval", "pull", "push")}
+    names = {"del_scan": "del_scan", "inval": "inval_closure", "pull": "pull_repair", "push": "push_closure"}
+    dominant = max(kern, key=lambda n: prof[n]["ms"])
+    rf = kern[dominant]
     roofline = None
     if rf:
         roofline = {
-            "kernel": f"{dominant}_closure" if dominant != "pull" else "pull_repair",
+            "kernel": names[dominant],
             "bound": "hbm", "achieved": rf["achieved_hbm_gbs"], "peak": hbm_peak, "unit": "GB/s",
             "frac": rf["achieved_hbm_gbs"] / hbm_peak, "traffic": None,
+            "traffic_source": None,
             "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
             "hbm_bytes_per_launch": rf["hbm_bytes"] / max(prof[dominant]["launches"], 1),
             "link_bytes_per_launch": rf["link_bytes"] / max(prof[dominant]["launches"], 1),
             "achieved_link_gbs": rf["achieved_link_gbs"], "link_peak_gbs": link_peak,
             "frac_of_combined_roofline": rf["frac_combined"],
+            "others": {names[k]: {"ms_per_batch": prof[k]["ms"] / args.steps, "achieved_hbm_gbs": v["achieved_hbm_gbs"],
+                                  "achieved_link_gbs": v["achieved_link_gbs"], "frac_combined": v["frac_combined"],
+                                  "hbm_bytes_per_launch": v["hbm_bytes"] / max(prof[k]["launches"], 1),
+                                  "link_bytes_per_launch": v["link_bytes"] / max(prof[k]["launches"], 1)}
+                       for k, v in kern.items() if v and k != dominant},
         }
 
+    if roofline:
+        ratio, src = traffic_ratio(roofline["kernel"])
+        if ratio:
+            roofline["traffic"] = ratio * roofline["hbm_bytes_per_launch"]
+            roofline["traffic_source"] = (f"ncu dram__bytes_read+write of {roofline['kernel']} on {src}, "
+                                          f"{ratio:.3f} x algorithmic HBM bytes, scaled to this launch "
+                                          f"(profiles/traffic.md)")
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -468,8 +517,248 @@ def run_queries(args):
     eng.close()
 
 
+def run_uneven(args):
+    """Update batches with sizes log-uniform in [1k, --uneven-max] (half
+    deletions, half insertions): the plain form (one cig_apply_batch_device
+    per batch, synchronised) against the batched form (all batches in one
+    cig_apply_batches_device call), each on a freshly loaded engine, with the
+    per-batch value digests compared."""
+    import torch
+
+    from coincgraph_b200 import Engine, gen
+
+    _, _, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    rng = np.random.default_rng(0xC01C1003)
+    sizes = np.exp(rng.uniform(np.log(1000), np.log(args.uneven_max), args.uneven_batches)).astype(np.int64)
+    symmetric = args.algo == "cc"
+    # symmetric streams come in (u,v)+(v,u) pairs: even phase sizes
+    half = np.maximum(sizes // 4 * 2, 2) if symmetric else np.maximum(sizes // 2, 1)
+    g, h = gen.rmat(args.scale, args.edge_factor, keep_handle=True, symmetric=symmetric)
+    ups = gen.updates(h, half, half, seed=gen.UPDATE_SEED_BASE + 3, symmetric=symmetric)
+    batches = [[torch.from_numpy(x.astype(np.int32)).to(dev) for x in ups.batch(i)] for i in range(len(sizes))]
+    res = {}
+    for form in ("plain", "batched"):
+        eng = Engine(args.algo, device=local, source=0, cache_gib=args.cache, max_batch=int(half.max()))
+        eng.load_csr(g.n, g.xadj, g.adj)
+        eng.init()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if form == "plain":
+            stats, digests = [], []
+            for b in batches:
+                stats.append(eng.apply_batch_device(*b))
+                digests.append(eng.digest())
+            wall = time.perf_counter() - t0 - 0.0
+        else:
+            stats, digests = eng.apply_batches_device(batches)
+            wall = time.perf_counter() - t0
+        dev_ms = [s.ms_delete + s.ms_insert + s.ms_cache for s in stats]
+        res[form] = {"wall_s": wall, "digests": digests, "batch_ms": dev_ms,
+                     "launches": sum(s.kernel_launches for s in stats)}
+        eng.close()
+    same = res["plain"]["digests"] == res["batched"]["digests"]
+    line = {
+        "metric": "batches/s, batched form vs plain per-batch form", "unit": "batches/s",
+        "value": len(sizes) / res["batched"]["wall_s"], "plain_value": len(sizes) / res["plain"]["wall_s"],
+        "speedup": res["plain"]["wall_s"] / res["batched"]["wall_s"], "digests_equal": same,
+        "n_gpus": 1, "higher_is_better": True, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"{args.algo.upper()} RMAT s{args.scale} ef{args.edge_factor}"
+                               f"{' symmetric' if symmetric else ''}, {len(sizes)} batches log-uniform "
+                               f"[1k, {args.uneven_max}] (half del, half ins), cache {args.cache} GiB",
+                   "sizes": sizes.tolist()},
+        "plain": {"wall_s": res["plain"]["wall_s"], "p50_ms": statistics.median(res["plain"]["batch_ms"]),
+                  "p99_ms": float(np.percentile(res["plain"]["batch_ms"], 99)), "launches": res["plain"]["launches"]},
+        "batched": {"wall_s": res["batched"]["wall_s"], "launches": res["batched"]["launches"],
+                    "device_ms_sum": sum(res["batched"]["batch_ms"])},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_served(args):
+    """A request stream (Poisson arrivals, or all at once) mixing update
+    batches of log-uniform sizes in [1k, --uneven-max] with BFS/SSSP queries
+    from uniform sources, served by cig_serve_* (waves, overlap) and by the
+    plain sequential form (one request at a time: cig_apply_batch, or a
+    one-source query), each on a freshly loaded engine.  Reports p50/p99
+    latency (arrival to result) and requests/s; query digests must agree."""
+    import torch
+
+    from coincgraph_b200 import Engine, gen
+
+    _, _, local = dist_env()
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(0xC01C1005)
+    nreq = args.requests
+    is_upd = rng.random(nreq) < args.update_frac
+    nupd = int(is_upd.sum())
+    sizes = np.exp(rng.uniform(np.log(1000), np.log(args.uneven_max), max(nupd, 1))).astype(np.int64)[:nupd]
+    half = np.maximum(sizes // 2, 1)
+    g, h = gen.rmat(args.scale, args.edge_factor, keep_handle=True)
+    ups = gen.updates(h, half, half, seed=gen.UPDATE_SEED_BASE + 5)
+    deg = np.diff(g.xadj.astype(np.int64))
+    live = np.flatnonzero(deg > 0)
+    reqs, ui = [], 0
+    for i in range(nreq):
+        if is_upd[i]:
+            reqs.append(("update", ups.batch(ui)))
+            ui += 1
+        else:
+            reqs.append(("bfs" if rng.random() < 0.5 else "sssp", int(rng.choice(live))))
+    gaps = rng.exponential(1.0 / args.rate, nreq) if args.rate > 0 else np.zeros(nreq)
+    arrive = np.cumsum(gaps)
+
+    def make_engine():
+        e = Engine("sssp", device=local, source=0, cache_gib=args.cache, max_batch=int(half.max()) if nupd else 0)
+        e.load_csr(g.n, g.xadj, g.adj)
+        e.init()
+        torch.cuda.synchronize()
+        return e
+
+    out = {}
+    # plain sequential form: one request at a time, in arrival order
+    eng = make_engine()
+    dev_out = torch.empty((1, g.n), dtype=torch.int32, device="cuda")
+    lat, digests = [], []
+    t0 = time.perf_counter()
+    for (kind, x), ta in zip(reqs, arrive):
+        now = time.perf_counter() - t0
+        if now < ta:
+            time.sleep(ta - now)
+        if kind == "update":
+            eng.apply_batch(*x)
+            digests.append(eng.digest())
+        else:
+            eng.query_device(kind, [x], dev_out, width=1)
+            row = dev_out.cpu().numpy().view(np.uint32)[0]
+            digests.append(int(row.astype(np.uint64).sum()))
+        lat.append((time.perf_counter() - t0 - ta) * 1e3)
+    out["plain"] = {"wall_s": time.perf_counter() - t0, "lat": lat}
+    plain_digests = digests
+    eng.close()
+    # served form
+    eng = make_engine()
+    eng.serve_start()
+    tickets = []
+    t0 = time.perf_counter()
+    for (kind, x), ta in zip(reqs, arrive):
+        now = time.perf_counter() - t0
+        if now < ta:
+            time.sleep(ta - now)
+        tickets.append(eng.submit_update(*x) if kind == "update" else eng.submit_query(kind, x))
+    res = [eng.wait(t) for t in tickets]
+    wall = time.perf_counter() - t0
+    eng.serve_stop()
+    eng.close()
+    lat_s = [r["done_ms"] - r["submit_ms"] for r in res]
+    waves = [r["wave"] for (k, _), r in zip(reqs, res) if k != "update"]
+    upd_ok = all(r["digest"] == d for (k, _), r, d in zip(reqs, res, plain_digests) if k == "update")
+    out["served"] = {"wall_s": wall, "lat": lat_s}
+
+    def pct(v, q):
+        return float(np.percentile(v, q)) if len(v) else None
+
+    def summary(form):
+        lat = out[form]["lat"]
+        ql = [x for (k, _), x in zip(reqs, lat) if k != "update"]
+        ul = [x for (k, _), x in zip(reqs, lat) if k == "update"]
+        return {"wall_s": out[form]["wall_s"], "requests_per_s": nreq / out[form]["wall_s"],
+                "update_batches_per_s": nupd / out[form]["wall_s"],
+                "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "query_p50_ms": pct(ql, 50),
+                "query_p99_ms": pct(ql, 99), "update_p50_ms": pct(ul, 50), "update_p99_ms": pct(ul, 99)}
+
+    line = {
+        "metric": "served request stream: requests/s and p50/p99 latency, served vs plain sequential",
+        "unit": "requests/s", "value": nreq / wall, "n_gpus": 1, "higher_is_better": True, "dtype": "u32",
+        "data": "synthetic",
+        "config": {"workload": f"RMAT s{args.scale} ef{args.edge_factor}, cache {args.cache} GiB, {nreq} requests "
+                               f"({nupd} update batches log-uniform [1k, {args.uneven_max}], the rest BFS/SSSP "
+                               f"queries), arrivals {'all at once' if args.rate <= 0 else f'Poisson {args.rate}/s'}"},
+        "served": summary("served"), "plain": summary("plain"),
+        "speedup_requests_per_s": out["plain"]["wall_s"] / wall,
+        "mean_wave": float(np.mean(waves)) if waves else None, "update_digests_equal": upd_ok,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_pr(args):
+    """Incremental PageRank (damping 0.85, per-vertex residual threshold
+    1e-9, so the FP64 L1 residual stays below 1e-9 x |V|): FP64 ranks and
+    FP32 ranks with Kahan-compensated sums on the same stream, each on a
+    freshly loaded engine; reports both batch rates and the FP32 ranks'
+    max-relative error against the FP64 ranks after every batch."""
+    import torch
+
+    from coincgraph_b200 import Engine, gen
+    from coincgraph_b200.engine import FLAG_PR_FP64
+
+    _, _, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    nb = args.warmup + args.steps
+    g, h = gen.rmat(args.scale, args.edge_factor, keep_handle=True)
+    ups = gen.updates(h, [args.batch] * nb, [args.batch] * nb, seed=gen.UPDATE_SEED_BASE + 4)
+    batches = [[torch.from_numpy(x.astype(np.int32)).to(dev) for x in ups.batch(i)] for i in range(nb)]
+    res = {}
+    for form, flags in (("fp64", FLAG_PR_FP64), ("fp32_kahan", 0)):
+        eng = Engine("pr", device=local, cache_gib=args.cache, pr_epsilon=1e-9, pr_max_rounds=100000, flags=flags,
+                     max_batch=args.batch)
+        eng.load_csr(g.n, g.xadj, g.adj)
+        t0 = time.perf_counter()
+        eng.init()
+        torch.cuda.synchronize()
+        init_s = time.perf_counter() - t0
+        init_rank = eng.pagerank(fp64=flags != 0)[0].astype(np.float64)
+        ms, l1, ranks = [], [], []
+        for i, b in enumerate(batches):
+            s = eng.apply_batch_device(*b)
+            if i >= args.warmup:
+                ms.append(s.ms_delete + s.ms_insert + s.ms_cache)
+                l1.append(s.pr_residual_l1)
+                ranks.append(eng.pagerank(fp64=flags != 0)[0].astype(np.float64))
+        res[form] = {"ms": ms, "l1": l1, "ranks": ranks, "init_s": init_s, "init_rank": init_rank}
+        eng.close()
+    err = [float(np.max(np.abs(a - b) / np.abs(b))) for a, b in zip(res["fp32_kahan"]["ranks"], res["fp64"]["ranks"])]
+    r32, r64 = res["fp32_kahan"]["init_rank"], res["fp64"]["init_rank"]
+    init_err = float(np.max(np.abs(r32 - r64) / np.abs(r64)))
+    line = {
+        "metric": "incremental PageRank batches/s, FP32+Kahan vs FP64 (max-rel error vs FP64)", "unit": "batches/s",
+        "value": args.steps / (sum(res["fp32_kahan"]["ms"]) * 1e-3),
+        "fp64_value": args.steps / (sum(res["fp64"]["ms"]) * 1e-3), "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "dtype": "f32+kahan / f64", "data": "synthetic",
+        "config": {"workload": f"PR RMAT s{args.scale} ef{args.edge_factor}, cache {args.cache} GiB, {args.batch} del "
+                               f"+ {args.batch} ins per batch, damping 0.85, per-vertex epsilon 1e-9",
+                   "vertices": g.n, "edges": g.m},
+        "max_rel_err_fp32_vs_fp64": max(err + [init_err]), "init_max_rel_err": init_err, "per_batch_max_rel_err": err,
+        "fp64_l1_residual_max": max(res["fp32_kahan"]["l1"]), "l1_bound": 1e-9 * g.n,
+        "p50_ms": {k: statistics.median(v["ms"]) for k, v in res.items()},
+        "p99_ms": {k: float(np.percentile(v["ms"], 99)) for k, v in res.items()},
+        "init_s": {k: v["init_s"] for k, v in res.items()},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
+    if args.workload == "pr":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the PR workload has no reference CPU arm here"}))
+            return
+        run_pr(args)
+        return
+    if args.workload == "served":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the served workload has no reference CPU arm"}))
+            return
+        run_served(args)
+        return
+    if args.workload == "uneven":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the uneven workload has no reference CPU arm"}))
+            return
+        run_uneven(args)
+        return
     if args.workload != "stream":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "query workloads have no reference CPU arm"}))

@@ -37,6 +37,8 @@
 #include <stdexcept>
 #include <string>
 #include <thread>
+
+#include <sys/stat.h>
 #include <vector>
 
 #include "cig.h"
@@ -141,6 +143,8 @@ static void define_flags() {
     def("top_ranks", 'i', "10", "(accepted, no effect)");
     def("print_ranks", 'b', "false", "(accepted, no effect)");
     def("device", 'i', "0", "CUDA device ordinal");
+    def("write_cigb", 'b', "false", "after parsing graphfile, write the binary sidecar graphfile.cigb");
+    def("autotune", 'b', "false", "choose the closures' launch shape on the loaded graph (cig_autotune)");
 #if defined(CIG_TOOL_PR)
     // samples/hybrid_pr/hybrid_pr.cu:21-24
     def("pr_max_batches", 'i', "10", "Maximum PR update batches (0 for static PR)");
@@ -151,6 +155,7 @@ static void define_flags() {
 #else
     // samples/hybrid_{bfs,sssp,cc}/*.cu:20-27
     def("source_node", 'i', "0", "The source node (clamped to [0, nnodes-1]; CC ignores it)");
+    def("weight_u255", 'b', "false", "SSSP: edge weights uniform in [1, 255] (extension; default (u+v)%128+1)");
     def("sparse", 'b', "false", "use async/push/dd + fusion for high-diameter (accepted, no effect)");
     def((std::string(kName) + "_max_batches").c_str(), 'i', "10", "Maximum number of update batches");
     def((std::string(kName) + "_print_checksum").c_str(), 'b', "false", "Print final checksums");
@@ -274,7 +279,53 @@ struct EdgeList {
     std::vector<uint32_t> src, dst;
 };
 
+// Binary sidecar `graphfile.cigb`: "CIGB0001", n (u32), m (u64), then the
+// m sources and m destinations (u32) in file order.  Read instead of the
+// text when it is at least as new as the text file; written by --write_cigb.
+static const char kCigbMagic[8] = {'C', 'I', 'G', 'B', '0', '0', '0', '1'};
+
+static bool read_cigb(const std::string &text_path, EdgeList &el) {
+    const std::string path = text_path + ".cigb";
+    struct stat st_t {}, st_b {};
+    if (::stat(path.c_str(), &st_b) != 0) return false;
+    if (::stat(text_path.c_str(), &st_t) == 0 && st_b.st_mtime < st_t.st_mtime) return false;
+    std::FILE *f = std::fopen(path.c_str(), "rb");
+    if (!f) return false;
+    char magic[8];
+    uint32_t n = 0;
+    uint64_t m = 0;
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kCigbMagic, 8) == 0 &&
+              std::fread(&n, sizeof(n), 1, f) == 1 && std::fread(&m, sizeof(m), 1, f) == 1;
+    if (ok) {
+        el.n = n;
+        el.src.resize(m);
+        el.dst.resize(m);
+        ok = std::fread(el.src.data(), sizeof(uint32_t), m, f) == m && std::fread(el.dst.data(), sizeof(uint32_t), m, f) == m;
+    }
+    std::fclose(f);
+    if (!ok) throw Fail("corrupt binary graph " + path);
+    for (uint64_t i = 0; i < m; ++i)
+        if (el.src[i] >= n || el.dst[i] >= n) throw Fail("binary graph " + path + " has an id >= n");
+    return true;
+}
+
+static void write_cigb(const std::string &text_path, const EdgeList &el) {
+    const std::string path = text_path + ".cigb";
+    std::FILE *f = std::fopen(path.c_str(), "wb");
+    if (!f) throw Fail("cannot write " + path);
+    const uint64_t m = el.src.size();
+    bool ok = std::fwrite(kCigbMagic, 1, 8, f) == 8 && std::fwrite(&el.n, sizeof(el.n), 1, f) == 1 &&
+              std::fwrite(&m, sizeof(m), 1, f) == 1 && std::fwrite(el.src.data(), sizeof(uint32_t), m, f) == m &&
+              std::fwrite(el.dst.data(), sizeof(uint32_t), m, f) == m;
+    ok = std::fclose(f) == 0 && ok;
+    if (!ok) throw Fail("cannot write " + path);
+}
+
 static EdgeList read_graph(const std::string &path) {
+    {
+        EdgeList el;
+        if (read_cigb(path, el)) return el;
+    }
     const std::vector<char> buf = read_file(path);
     const char *base = buf.data();
     const size_t size = buf.size();
@@ -408,8 +459,19 @@ static Csr export_graph(uint32_t n) {
     return g;
 }
 
+static bool g_weight_u255 = false;  // --weight_u255 (hybrid_sssp)
+
 static uint64_t weight(uint32_t u, uint32_t v) {
 #if defined(CIG_TOOL_SSSP)
+    if (g_weight_u255) {  // the library's CIG_FLAG_WEIGHT_U255 function (lowbias32, C. Wellons)
+        uint32_t x = u * 0x9E3779B1u + v * 0x85EBCA77u;
+        x ^= x >> 16;
+        x *= 0x7FEB352Du;
+        x ^= x >> 15;
+        x *= 0x846CA68Bu;
+        x ^= x >> 16;
+        return 1u + x % 255u;
+    }
     return (static_cast<uint64_t>(u) + v) % 128 + 1;
 #else
     (void)u;
@@ -602,6 +664,7 @@ static bool run() {
     Stopwatch sw_load(true);
     EdgeList el = read_graph(graphfile);
     if (el.n == 0) throw Fail(std::string(kUpper) + " requires a nonempty graph");
+    if (B("write_cigb")) write_cigb(graphfile, el);
     Updates up;
     if (have_updates && max_batches_flag > 0) up = read_updates(S("updatefile"), S("update_size"));
 
@@ -616,6 +679,10 @@ static bool run() {
     o.pr_max_rounds = static_cast<int32_t>(max_rounds);
     if (B("pr_fp64")) o.flags |= CIG_FLAG_PR_FP64;
 #else
+#if defined(CIG_TOOL_SSSP)
+    g_weight_u255 = B("weight_u255");
+    if (g_weight_u255) o.flags |= CIG_FLAG_WEIGHT_U255;
+#endif
     const long long src_flag = I("source_node");
     o.source = static_cast<uint32_t>(std::min<long long>(std::max<long long>(0, src_flag), el.n - 1));
 #endif
@@ -640,6 +707,14 @@ static bool run() {
     Stopwatch sw_init(true);
     ck(cig_init(g_h), "cig_init");
     sw_init.stop();
+#if !defined(CIG_TOOL_PR)
+    if (B("autotune")) {
+        cig_tune_result tr;
+        ck(cig_autotune(g_h, &tr), "cig_autotune");
+        LOG("[AUTOTUNE] blocks_per_sm=%u split_degree=%u solve_ms=%.3f candidates=%u\n", tr.blocks_per_sm,
+            tr.split_degree, tr.best_ms, tr.candidates);
+    }
+#endif
     bool success = true;
 #if defined(CIG_TOOL_PR)
     LOG("[PR-INITIAL] compute_ms=%.3f alpha=0.85 base=0.15 dangling=drop\n", sw_init.ms());

@@ -92,7 +92,7 @@ struct Status {
     uint32_t err_info;
     uint32_t barrier_count;
     uint32_t barrier_gen;
-    unsigned long long counters[32];
+    unsigned long long counters[40];
 };
 
 enum Counter : int {
@@ -116,6 +116,10 @@ enum Counter : int {
     kCntInval = 20,
     kCntPull = 24,
     kCntPr = 28,
+    // Flat deletion scan (forward and reverse rows): row entries read, of
+    // which from HBM.
+    kCntDelScanned = 32,
+    kCntDelScannedCached = 33,
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
@@ -196,12 +200,29 @@ __device__ __forceinline__ bool grid_barrier(Status *st) {
 // Edge weights of the reference samples: BFS 1 (samples/hybrid_bfs/
 // hybrid_bfs.cu:41-47), SSSP (src+dst)%128+1 (include/framework/variants/
 // api.cuh:26-28), CC 0 (samples/hybrid_cc/hybrid_cc.cu:51-57).
-enum Algo : int { kBfs = 0, kSssp = 1, kCc = 2, kPr = 3 };
+// kSsspU: SSSP with weights uniform in [1, 255] (CIG_FLAG_WEIGHT_U255).
+enum Algo : int { kBfs = 0, kSssp = 1, kCc = 2, kPr = 3, kSsspU = 4 };
+
+// Weight of edge (u, v) in [1, 255] for kSsspU: 1 + lowbias32(u*G + v*H)
+// mod 255, where lowbias32 is C. Wellons' published 32-bit integer hash
+// ("Prospecting for hash functions", 2018).  A function of the edge, so the
+// weight needs no storage and moves with the row; the reference itself never
+// stores file weights (its chunk store holds destinations only).
+__host__ __device__ __forceinline__ uint32_t weight_u255(uint32_t u, uint32_t v) {
+    uint32_t x = u * 0x9E3779B1u + v * 0x85EBCA77u;
+    x ^= x >> 16;
+    x *= 0x7FEB352Du;
+    x ^= x >> 15;
+    x *= 0x846CA68Bu;
+    x ^= x >> 16;
+    return 1u + x % 255u;
+}
 
 template <int A>
 __device__ __forceinline__ uint32_t edge_weight(uint32_t u, uint32_t v) {
     if (A == kBfs) return 1u;
     if (A == kCc) return 0u;
+    if (A == kSsspU) return weight_u255(u, v);
     return ((u + v) & 127u) + 1u;  // (u+v) mod 2^32 keeps the residue mod 128
 }
 

@@ -13,18 +13,26 @@
 #include <atomic>
 #include <cstdio>
 #include <cstdlib>
+#include <chrono>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
 #include <new>
 #include <stdexcept>
 #include <string>
 #include <thread>
 #include <type_traits>
+#include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include "../../include/cig.h"
+#include "cache.cuh"
 #include "common.cuh"
 #include "expand.cuh"
 #include "mutate.cuh"
@@ -178,6 +186,8 @@ enum SmallIdx : int {
     kBigRows = 13,  // 3 counters of deferred hub rows
     kCompactCount = 16,
     kOrderedCount = 17,
+    kGaF = 18,  // addition-phase group counts of a presorted batch
+    kGaR = 19,
     kSmallCount = 20
 };
 
@@ -239,6 +249,19 @@ struct cig_handle {
     uint64_t cache_slots = 0;
     uint64_t resident = 0;
     uint32_t *seg_hot = nullptr;
+    // Segment table service (cache.cuh); off with CIG_FLAG_NO_CACHE_REFRESH.
+    bool refresh = false;
+    int32_t *slot_seg = nullptr;
+    uint32_t *seg_score = nullptr, *free_slots = nullptr, *seg_victims = nullptr, *seg_admits = nullptr;
+    uint32_t *seg_ctl = nullptr;
+    SegTable seg_table() const {
+        return SegTable{fwd.seg_slot, slot_seg, fwd.seg_dirty, seg_score, seg_hot, free_slots, seg_victims,
+                        seg_admits, seg_ctl, static_cast<uint32_t>(cache_slots), static_cast<uint32_t>(fwd.seg_total),
+                        admit_score, cold_score};
+    }
+    // Service thresholds; CIG_CACHE_ADMIT_SCORE / CIG_CACHE_COLD_SCORE
+    // override them when the graph is loaded.
+    uint32_t admit_score = kAdmitScore, cold_score = kColdScore;
 
     unsigned long long *state = nullptr;
     uint32_t *qstamp = nullptr, *aff_stamp = nullptr, *q0 = nullptr, *q1 = nullptr, *list = nullptr;
@@ -250,6 +273,10 @@ struct cig_handle {
     uint32_t epoch = 0;
 
     void *pr_rank = nullptr, *pr_res = nullptr, *pr_contrib = nullptr, *pr_amend = nullptr;
+    double *pr_amend64 = nullptr;  // FP32 mode: per-vertex FP64 amend accumulator (pr_amend_fold)
+    uint32_t *pr_hub_bits = nullptr, *pr_hub_prefix = nullptr;  // FP32 mode: FP64 residual slots (pr.cuh)
+    uint32_t pr_hubs = 0;
+    double *pr_res_hub = nullptr;
     float *pr_comp = nullptr;
     uint32_t *pr_queued = nullptr;
     bool pr64 = false;
@@ -264,8 +291,23 @@ struct cig_handle {
     // flat deletion: per-group chunk counts, their inclusive prefix sum, the
     // groups left to the ordered kernels, first match per key
     uint32_t *chunks = nullptr, *chunk_end = nullptr, *ordered = nullptr, *firstpos = nullptr;
+    uint32_t *chunk_map = nullptr;  // group of every 512-entry scan chunk
+    uint64_t chunk_map_cap = 0;
+    int del_scan_per_sm = 0;
+    int del_scan_blocks_per_sm() {
+        if (!del_scan_per_sm) {
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&del_scan_per_sm, del_scan, kMutWarps * 32, 0));
+            del_scan_per_sm = std::max(1, del_scan_per_sm);
+        }
+        return del_scan_per_sm;
+    }
     // group building: head flags, their exclusive scan, group ends per direction
     uint32_t *gflags = nullptr, *gpos = nullptr, *gendf = nullptr, *gendr = nullptr;
+    // whole-batch sort (apply_batch): packed keys, and the addition phase's
+    // groups, kept apart from the deletion phase's
+    unsigned long long *kc = nullptr, *tc = nullptr;
+    uint32_t *gaf = nullptr, *gar = nullptr, *gaendf = nullptr, *gaendr = nullptr;
+    bool presorted = false;
     void *cub = nullptr;
     size_t cub_bytes = 0;
     uint32_t *stage = nullptr;  // pinned staging for host update arrays (4 * bcap)
@@ -325,6 +367,8 @@ struct cig_handle {
             prof[g.first].rows += c[g.second + 2];
             prof[g.first].hits += c[g.second + 3];
         }
+        prof[CIG_STAGE_DEL_SCAN].edges += c[kCntDelScanned];
+        prof[CIG_STAGE_DEL_SCAN].edges_cached += c[kCntDelScannedCached];
     }
 
     // ------------------------------------------------------------ helpers
@@ -340,21 +384,26 @@ struct cig_handle {
     // Deferred hub rows; the counters are cleared before every launch that uses them.
     BigList big_list() {
         CK(cudaMemsetAsync(small + kBigRows, 0, 3 * sizeof(uint32_t), stream));
-        return BigList{big_rows, small + kBigRows, kBigRowCap};
+        return BigList{big_rows, small + kBigRows, kBigRowCap, tune.split};
     }
 
     template <class K>
     int coop_blocks(K kernel, int tpb) const {
         int per_sm = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, tpb, 0));
-        int want = 4;
-        if (const char *e = std::getenv("CIG_COOP_BLOCKS_PER_SM")) want = std::max(1, std::atoi(e));
-        per_sm = std::min(per_sm, want);
+        per_sm = std::min(per_sm, static_cast<int>(tune.per_sm));
         if (per_sm < 1) throw CigError(CIG_ERR_DEVICE, "cooperative kernel does not fit on an SM");
         return per_sm * sms;
     }
 
     uint64_t n_launch = 0;  // kernels this engine launched (CUB sort kernels not included)
+
+    // Launch-shape parameters of the persistent closures, chosen by
+    // cig_autotune (or CIG_COOP_BLOCKS_PER_SM / CIG_SPLIT_DEG at create).
+    struct Tune {
+        uint32_t per_sm = 4;        // cooperative blocks per SM (frontier tile = per_sm x 148 blocks)
+        uint32_t split = kSplitDeg; // rows of at least this many entries are expanded by the whole grid
+    } tune;
 
     template <class... P>
     void launch(void (*kernel)(P...), int grid, int block, typename Identity<P>::type... args) {
@@ -386,6 +435,7 @@ struct cig_handle {
     uint64_t launch_mark = 0;
 
     void reset_counters() {
+        presorted = false;
         CK(cudaMemsetAsync(status->counters, 0, sizeof(status->counters), stream));
         launch_mark = n_launch;
     }
@@ -422,7 +472,12 @@ struct cig_handle {
     void dispatch(F f) {
         switch (opt.algo) {
         case CIG_BFS: f(std::integral_constant<int, kBfs>{}); break;
-        case CIG_SSSP: f(std::integral_constant<int, kSssp>{}); break;
+        case CIG_SSSP:
+            if (opt.flags & CIG_FLAG_WEIGHT_U255)
+                f(std::integral_constant<int, kSsspU>{});
+            else
+                f(std::integral_constant<int, kSssp>{});
+            break;
         case CIG_CC: f(std::integral_constant<int, kCc>{}); break;
         default: throw CigError(CIG_ERR_ARG, "algorithm has no traversal state");
         }
@@ -450,6 +505,8 @@ struct cig_handle {
         dmalloc(tags, 1);
         CK(cudaMemset(tags, 0, sizeof(TagState)));
         pr64 = (opt.flags & CIG_FLAG_PR_FP64) != 0;
+        if (const char *e = std::getenv("CIG_COOP_BLOCKS_PER_SM")) tune.per_sm = std::max(1, std::atoi(e));
+        if (const char *e = std::getenv("CIG_SPLIT_DEG")) tune.split = std::max(32, std::atoi(e));
     }
 
     void destroy() {
@@ -469,6 +526,12 @@ struct cig_handle {
         dfree(rev.dev);
         dfree(rev.alloc);
         dfree(seg_hot);
+        dfree(slot_seg);
+        dfree(seg_score);
+        dfree(free_slots);
+        dfree(seg_victims);
+        dfree(seg_admits);
+        dfree(seg_ctl);
         dfree(state);
         dfree(qstamp);
         dfree(aff_stamp);
@@ -485,10 +548,19 @@ struct cig_handle {
         dfree(pr_res);
         dfree(pr_contrib);
         dfree(pr_amend);
+        dfree(pr_amend64);
+        dfree(pr_hub_bits);
+        dfree(pr_hub_prefix);
+        dfree(pr_res_hub);
         dfree(pr_comp);
         dfree(pr_queued);
         free_batch();
         dfree(tmp_u32);
+        dfree(chunk_map);
+        dfree(bsnap);
+        dfree(bdig);
+        for (auto &e : bev) cudaEventDestroy(e);
+        bev.clear();
         free_queries();
         if (stream) cudaStreamDestroy(stream);
     }
@@ -508,6 +580,12 @@ struct cig_handle {
         dfree(mr);
         dfree(bigf);
         dfree(bigr);
+        dfree(kc);
+        dfree(tc);
+        dfree(gaf);
+        dfree(gar);
+        dfree(gaendf);
+        dfree(gaendr);
         dfree(pf);
         dfree(prr);
         dfree(touched);
@@ -554,21 +632,27 @@ struct cig_handle {
         dmalloc(chunk_end, cap);
         dmalloc(ordered, cap);
         dmalloc(firstpos, cap);
-        dmalloc(gflags, cap);
-        dmalloc(gpos, cap);
+        dmalloc(gflags, 4 * cap);
+        dmalloc(gpos, 4 * cap);
         dmalloc(gendf, cap);
         dmalloc(gendr, cap);
+        dmalloc(kc, 4 * cap);
+        dmalloc(tc, 4 * cap);
+        dmalloc(gaf, cap);
+        dmalloc(gar, cap);
+        dmalloc(gaendf, cap);
+        dmalloc(gaendr, cap);
         if (opt.algo == CIG_PR) {
             dfree(pr_amend);
-            CK(cudaMalloc(&pr_amend, 2 * cap * (pr64 ? sizeof(double) : sizeof(float))));
+            CK(cudaMalloc(&pr_amend, 2 * cap * sizeof(double)));
         }
-        cub::DoubleBuffer<unsigned long long> db(kf, t1);
+        cub::DoubleBuffer<unsigned long long> db(kc, tc);
         size_t bytes = 0;
-        CK(cub::DeviceRadixSort::SortKeys(nullptr, bytes, db, static_cast<int>(cap), 0, 64, stream));
+        CK(cub::DeviceRadixSort::SortKeys(nullptr, bytes, db, static_cast<int>(4 * cap), 0, 64, stream));
         size_t scan_bytes = 0;
         CK(cub::DeviceScan::InclusiveSum(nullptr, scan_bytes, chunks, chunk_end, static_cast<int>(cap), stream));
         bytes = std::max(bytes, scan_bytes);
-        CK(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, gflags, gpos, static_cast<int>(cap), stream));
+        CK(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, gflags, gpos, static_cast<int>(4 * cap), stream));
         bytes = std::max(bytes, scan_bytes);
         cub_bytes = bytes;
         CK(cudaMalloc(&cub, std::max<size_t>(bytes, 16)));
@@ -653,14 +737,17 @@ struct cig_handle {
         } else {
             budget_slots = opt.cache_gib > 0 ? static_cast<uint64_t>(opt.cache_gib * 1073741824.0 / 4.0) : 0;
         }
-        // Slots left over after the used segments go to the headroom segments
-        // that the block allocator hands out later, so relocated rows land in
-        // HBM while the budget lasts.
+        // Slots beyond the used segments serve the segments that the block
+        // allocator hands out later: with the segment-table service they sit
+        // on its free stack, without it they are bound to the headroom
+        // segments in order.  Either way relocated rows land in HBM while the
+        // budget lasts.
         cache_slots = std::min<uint64_t>(budget_slots >> kSegShift, fwd.seg_total);
-        resident = cache_slots;
+        refresh = cache_slots > 0 && !(opt.flags & CIG_FLAG_NO_CACHE_REFRESH);
+        const uint64_t filled = std::min<uint64_t>(cache_slots, fwd.seg_used);
+        resident = refresh ? filled : cache_slots;
         if (cache_slots) {
             dmalloc(fwd.dev, cache_slots * kSegEdges);
-            const uint64_t filled = std::min<uint64_t>(cache_slots, fwd.seg_used);
             if (filled)
                 CK(cudaMemcpy(fwd.dev, fwd.host, filled * kSegEdges * sizeof(uint32_t), cudaMemcpyHostToDevice));
         }
@@ -674,6 +761,26 @@ struct cig_handle {
         }
         dmalloc(seg_hot, fwd.seg_total);
         CK(cudaMemset(seg_hot, 0, fwd.seg_total * sizeof(uint32_t)));
+        if (refresh) {
+            if (const char *e = std::getenv("CIG_CACHE_ADMIT_SCORE")) admit_score = static_cast<uint32_t>(std::atol(e));
+            if (const char *e = std::getenv("CIG_CACHE_COLD_SCORE")) cold_score = static_cast<uint32_t>(std::atol(e));
+            std::vector<int32_t> owner(cache_slots, -1);
+            for (uint64_t s = 0; s < filled; ++s) owner[s] = static_cast<int32_t>(s);
+            std::vector<uint32_t> stack;
+            for (uint64_t k = cache_slots; k-- > filled;) stack.push_back(static_cast<uint32_t>(k));
+            dmalloc(slot_seg, cache_slots);
+            CK(cudaMemcpy(slot_seg, owner.data(), cache_slots * sizeof(int32_t), cudaMemcpyHostToDevice));
+            dmalloc(free_slots, cache_slots);
+            if (!stack.empty())
+                CK(cudaMemcpy(free_slots, stack.data(), stack.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+            dmalloc(seg_score, fwd.seg_total);
+            CK(cudaMemset(seg_score, 0, fwd.seg_total * sizeof(uint32_t)));
+            dmalloc(seg_victims, kMaxEvict);
+            dmalloc(seg_admits, kMaxAdmit);
+            const uint32_t ctl[kCtlCount] = {static_cast<uint32_t>(stack.size()), static_cast<uint32_t>(fwd.seg_used)};
+            dmalloc(seg_ctl, kCtlCount);
+            CK(cudaMemcpy(seg_ctl, ctl, sizeof(ctl), cudaMemcpyHostToDevice));
+        }
 
         // Reverse arena (device only) for deletion repair.
         if (opt.algo != CIG_PR) build_reverse(xadj, adj, m);
@@ -687,7 +794,36 @@ struct cig_handle {
             CK(cudaMalloc(&pr_rank, n * es));
             CK(cudaMalloc(&pr_res, n * es));
             CK(cudaMalloc(&pr_contrib, (n + 1) * es));
-            if (!pr64) dmalloc(pr_comp, n);
+            if (!pr64) {
+                dmalloc(pr_comp, n);
+                dmalloc(pr_amend64, n);
+                CK(cudaMemset(pr_amend64, 0, n * sizeof(double)));
+                // FP64 residual slots for vertices of in-degree >= kPrHubInDeg.
+                std::vector<std::atomic<uint32_t>> indeg(n);
+                parallel_for(m, [&](uint64_t b, uint64_t e) {
+                    for (uint64_t i = b; i < e; ++i) indeg[adj[i]].fetch_add(1, std::memory_order_relaxed);
+                });
+                uint64_t hub_deg = kPrHubInDeg;
+                if (const char *e = std::getenv("CIG_PR_HUB_INDEG")) hub_deg = std::strtoull(e, nullptr, 10);
+                const uint32_t words = (n + 31) / 32;
+                std::vector<uint32_t> bits(words, 0), prefix(words, 0);
+                uint32_t nh = 0;
+                for (uint32_t w = 0; w < words; ++w) {
+                    prefix[w] = nh;
+                    for (uint32_t k = 0; k < 32 && 32 * w + k < n; ++k)
+                        if (indeg[32 * w + k].load(std::memory_order_relaxed) >= hub_deg) {
+                            bits[w] |= 1u << k;
+                            ++nh;
+                        }
+                }
+                dmalloc(pr_hub_bits, words);
+                dmalloc(pr_hub_prefix, words);
+                CK(cudaMemcpy(pr_hub_bits, bits.data(), words * sizeof(uint32_t), cudaMemcpyHostToDevice));
+                CK(cudaMemcpy(pr_hub_prefix, prefix.data(), words * sizeof(uint32_t), cudaMemcpyHostToDevice));
+                dmalloc(pr_res_hub, std::max<uint32_t>(nh, 1));
+                CK(cudaMemset(pr_res_hub, 0, std::max<uint32_t>(nh, 1) * sizeof(double)));
+                pr_hubs = nh;
+            }
             dmalloc(pr_queued, n);
             dmalloc(aff_stamp, n);
             CK(cudaMemset(aff_stamp, 0, n * sizeof(uint32_t)));
@@ -757,20 +893,23 @@ struct cig_handle {
             else
                 pr_init_run<float>();
         } else {
-            dispatch([&](auto tag) {
-                constexpr int A = decltype(tag)::value;
-                launch(init_state<A>, persistent_grid(), 256, state, n, source);
-                CK(cudaMemsetAsync(small + kFr, 0, 3 * sizeof(uint32_t), stream));
-                if (A == kCc)
-                    launch(enqueue_all_nonempty, persistent_grid(), 256, fwd.desc, n, frontier(), status);
-                else
-                    launch(set_single, 1, 1, q0, small + kFr, source);
-                check_launch();
-                run_push<A>();
-            });
+            dispatch([&](auto tag) { static_solve<decltype(tag)::value>(); });
         }
         finish();
         initialized = true;
+    }
+
+    // The static solve from scratch (Start, framework.cuh:1151-1182).
+    template <int A>
+    void static_solve() {
+        launch(init_state<A>, persistent_grid(), 256, state, n, source);
+        CK(cudaMemsetAsync(small + kFr, 0, 3 * sizeof(uint32_t), stream));
+        if (A == kCc)
+            launch(enqueue_all_nonempty, persistent_grid(), 256, fwd.desc, n, frontier(), status);
+        else
+            launch(set_single, 1, 1, q0, small + kFr, source);
+        check_launch();
+        run_push<A>();
     }
 
     template <int A>
@@ -784,8 +923,9 @@ struct cig_handle {
     // ------------------------------------------------------------ PR
     template <class T>
     PrArrays<T> pr_arrays() {
-        return PrArrays<T>{static_cast<T *>(pr_rank), static_cast<T *>(pr_res), pr_comp, pr_queued, q0, q1,
-                           small + kFr, static_cast<T *>(pr_contrib), small + kFinalRound, n + 1};
+        return PrArrays<T>{static_cast<T *>(pr_rank), static_cast<T *>(pr_res), pr_hub_bits, pr_hub_prefix, pr_res_hub,
+                           pr_comp, pr_queued, q0, q1, small + kFr, static_cast<T *>(pr_contrib), small + kFinalRound,
+                           n + 1};
     }
 
     template <class T>
@@ -809,7 +949,7 @@ struct cig_handle {
         launch(pr_normalize_frontier<T>, persistent_grid(), 256, a);
         launch(pr_set_counts<T>, 1, 1, a);
         CK(cudaMemsetAsync(small64, 0, sizeof(double), stream));
-        launch(pr_residual_l1<T>, persistent_grid(), 256, static_cast<const T *>(pr_res), n,
+        launch(pr_residual_l1<T>, persistent_grid(), 256, pr_arrays<T>(), n,
                                                                   reinterpret_cast<double *>(small64));
         check_launch();
     }
@@ -826,24 +966,30 @@ struct cig_handle {
                                                                   static_cast<uint32_t>(na), n, aff_stamp, epoch,
                                                                   touched, small + kTouched,
                                                                   static_cast<uint32_t>(2 * bcap), status);
-        T *amend = static_cast<T *>(pr_amend);
         // r' = r + alpha (P_new^T - P_old^T) x over the touched sources.
-        int p = prof_begin(CIG_STAGE_PR);
-        launch(pr_amend_contrib<T>, persistent_grid(), 256, fwd.desc, a, touched, small + kTouched, T(-1),
-                                                                   amend);
-        launch(pr_amend_scatter<T>, persistent_grid(), kTpbPr, fwd.view(), a, touched, small + kTouched,
-                                                                      amend, eps, status);
-        prof_end(p);
-        check_launch();
+        auto amend_pass = [&](double sign) {
+            const int p = prof_begin(CIG_STAGE_PR);
+            if (sizeof(T) == 4) {
+                double *c64 = static_cast<double *>(pr_amend);
+                launch(pr_amend_contrib64<T>, persistent_grid(), 256, fwd.desc, a, touched, small + kTouched, sign,
+                       c64);
+                launch(pr_amend_scatter64<T>, persistent_grid(), kTpbPr, fwd.view(), touched, small + kTouched, c64,
+                       pr_amend64, status);
+            } else {
+                T *amend = static_cast<T *>(pr_amend);
+                launch(pr_amend_contrib<T>, persistent_grid(), 256, fwd.desc, a, touched, small + kTouched,
+                       static_cast<T>(sign), amend);
+                launch(pr_amend_scatter<T>, persistent_grid(), kTpbPr, fwd.view(), a, touched, small + kTouched,
+                       amend, eps, status);
+            }
+            prof_end(p);
+            check_launch();
+        };
+        amend_pass(-1.0);
         mutate_forward_delete(d_du, d_dv, nd, true);
         mutate_forward_add(d_au, d_av, na, true);
-        p = prof_begin(CIG_STAGE_PR);
-        launch(pr_amend_contrib<T>, persistent_grid(), 256, fwd.desc, a, touched, small + kTouched, T(1),
-                                                                   amend);
-        launch(pr_amend_scatter<T>, persistent_grid(), kTpbPr, fwd.view(), a, touched, small + kTouched,
-                                                                      amend, eps, status);
-        prof_end(p);
-        check_launch();
+        amend_pass(1.0);
+        if (sizeof(T) == 4) launch(pr_amend_fold<T>, persistent_grid(), 256, a, pr_amend64, n, eps, status);
         pr_run_converge<T>();
     }
 
@@ -868,6 +1014,130 @@ struct cig_handle {
         return Groups{start, end, gcount};
     }
 
+    // Time the static solve (the heaviest closure, from scratch) for every
+    // candidate launch shape and keep the fastest.  The solve's values are
+    // unique, so re-running it leaves the maintained values unchanged; the
+    // last run uses the chosen shape.
+    void autotune(cig_tune_result *res) {
+        require_ready();
+        if (opt.algo == CIG_PR) throw CigError(CIG_ERR_ARG, "autotune covers the BFS/SSSP/CC closures");
+        const uint32_t per_sm_c[] = {2, 4, 8};
+        const uint32_t split_c[] = {1024, 4096, 16384};
+        Tune best = tune;
+        float best_ms = 1e30f;
+        uint32_t tried = 0;
+        for (uint32_t ps : per_sm_c) {
+            for (uint32_t sp : split_c) {
+                tune.per_sm = ps;
+                tune.split = sp;
+                float ms = 0;
+                for (int rep = 0; rep < 2; ++rep) {  // first run warms caches and occupancy queries
+                    CK(cudaEventRecord(ev[0], stream));
+                    dispatch([&](auto tag) { static_solve<decltype(tag)::value>(); });
+                    CK(cudaEventRecord(ev[1], stream));
+                    finish();
+                    CK(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+                }
+                ++tried;
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = tune;
+                }
+            }
+        }
+        tune = best;
+        dispatch([&](auto tag) { static_solve<decltype(tag)::value>(); });
+        finish();
+        if (res) {
+            std::memset(res, 0, sizeof(*res));
+            res->blocks_per_sm = best.per_sm;
+            res->split_degree = best.split;
+            res->best_ms = best_ms;
+            res->candidates = tried;
+        }
+    }
+
+    void run_cache_service() {
+        const int p = prof_begin(CIG_STAGE_CACHE);
+        cache_service();
+        prof_end(p);
+    }
+
+    // Per-batch residency decisions of the segment table (cache.cuh), on the
+    // engine stream after the insertion phase.
+    void cache_service() {
+        if (!refresh) return;
+        const SegTable t = seg_table();
+        CK(cudaMemsetAsync(seg_ctl + kCtlVictims, 0, 2 * sizeof(uint32_t), stream));
+        launch(seg_rescore, grid_for(fwd.seg_total), 256, t, static_cast<uint32_t>(fwd.seg_total), kMaxEvict);
+        launch(seg_plan, 1, 32, t);
+        launch(seg_evict, static_cast<int>(std::min<uint64_t>(kMaxEvict, sms * 4)), 256, t, fwd.dev, fwd.host_dptr,
+               status);
+        launch(seg_admit, static_cast<int>(kMaxAdmit), 256, t, fwd.dev, fwd.host_dptr, status);
+        check_launch();
+    }
+
+    // Sort the keys of a whole batch at once (PackedSets): fills kf/kr (forward
+    // and reverse deletion keys), t1/t2 (addition keys) and their groups, and
+    // sets `presorted` for the two phases that follow.  Returns false (and
+    // leaves the per-phase sorts to the phases) when the fields do not fit.
+    bool presort_batch(const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd, const uint32_t *d_au,
+                       const uint32_t *d_av, uint64_t na) {
+        const uint64_t mx = std::max<uint64_t>(n, std::max(nd, na));
+        uint32_t f = 0;
+        while (f < 32 && (1ull << f) <= mx) ++f;
+        if (2 + 2 * f > 64) return false;
+        PackedSets ps{};
+        ps.off[0] = 0;
+        ps.off[1] = static_cast<uint32_t>(nd);
+        ps.off[2] = static_cast<uint32_t>(2 * nd);
+        ps.off[3] = static_cast<uint32_t>(2 * nd + na);
+        ps.off[4] = static_cast<uint32_t>(2 * nd + 2 * na);
+        ps.f = f;
+        const uint64_t total = ps.off[4];
+        const int p = prof_begin(CIG_STAGE_GROUP);
+        CK(cudaMemsetAsync(small + kGcF, 0, 2 * sizeof(uint32_t), stream));
+        CK(cudaMemsetAsync(small + kGaF, 0, 2 * sizeof(uint32_t), stream));
+        if (total) {
+            launch(make_keys_batch, grid_for(total), 256, d_du, d_dv, static_cast<uint32_t>(nd), d_au, d_av,
+                   static_cast<uint32_t>(na), n, ps, kc, status);
+            const unsigned long long *sorted;
+            size_t bytes = cub_bytes;
+            // ~0 pads the small sort's tail: keys of 2 + 2F < 64 bits sort below it.
+            if (total <= kSmallSortKeys) {
+                launch(sort_small, 1, kSmallSortThreads, kc, static_cast<uint32_t>(total), 2 + 2 * static_cast<int>(f),
+                       tc);
+                sorted = tc;
+            } else {
+                cub::DoubleBuffer<unsigned long long> db(kc, tc);
+                CK(cub::DeviceRadixSort::SortKeys(cub, bytes, db, static_cast<int>(total), 0,
+                                                  2 + 2 * static_cast<int>(f), stream));
+                sorted = db.Current();
+            }
+            launch(unpack_keys_batch, grid_for(total), 256, sorted, ps, kf, kr, t1, t2, gflags);
+            bytes = cub_bytes;
+            CK(cub::DeviceScan::ExclusiveSum(cub, bytes, gflags, gpos, static_cast<int>(total), stream));
+            SetGroups sg{};
+            sg.start[0] = gf;
+            sg.end[0] = gendf;
+            sg.count[0] = small + kGcF;
+            sg.start[1] = gr;
+            sg.end[1] = gendr;
+            sg.count[1] = small + kGcR;
+            sg.start[2] = gaf;
+            sg.end[2] = gaendf;
+            sg.count[2] = small + kGaF;
+            sg.start[3] = gar;
+            sg.end[3] = gaendr;
+            sg.count[3] = small + kGaR;
+            launch(group_scatter_batch, grid_for(total), 256, sorted, ps, gflags, gpos, sg);
+        }
+        prof_end(p);
+        check_launch();
+        presorted = true;
+        return true;
+    }
+
     void mutate_delete_arena(DevArena &A, const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd, bool forward,
                              bool with_stats) {
         if (nd == 0) return;
@@ -880,15 +1150,19 @@ struct cig_handle {
         uint32_t *gcount = small + (forward ? kGcF : kGcR);
         uint32_t *bcount = small + (forward ? kBigF : kBigR);
         int p = prof_begin(CIG_STAGE_GROUP);
-        // make_keys_del fills both kf and kr; only build them once per phase.
-        if (forward || opt.algo == CIG_PR) {
-            launch(make_keys_del, grid_for(nd), 256, d_du, d_dv, m, n, kf, kr, status);
-            check_launch();
+        unsigned long long *sorted = keys;
+        Groups grp{groups, forward ? gendf : gendr, gcount};
+        if (!presorted) {
+            // make_keys_del fills both kf and kr; only build them once per phase.
+            if (forward || opt.algo == CIG_PR) {
+                launch(make_keys_del, grid_for(nd), 256, d_du, d_dv, m, n, kf, kr, status);
+                check_launch();
+            }
+            sorted = sort_keys(keys, tmp, nd);
+            grp = build_groups(sorted, nd, groups, forward ? gendf : gendr, gcount);
         }
-        unsigned long long *sorted = sort_keys(keys, tmp, nd);
         CK(cudaMemsetAsync(bcount, 0, sizeof(uint32_t), stream));
         CK(cudaMemsetAsync(matched, 0, nd * sizeof(uint32_t), stream));
-        const Groups grp = build_groups(sorted, nd, groups, forward ? gendf : gendr, gcount);
         prof_end(p);
         p = prof_begin(forward ? CIG_STAGE_MUTATE : CIG_STAGE_MUTATE_REV);
         unsigned long long *stats = with_stats ? status->counters : nullptr;
@@ -904,7 +1178,22 @@ struct cig_handle {
             size_t bytes = cub_bytes;
             CK(cub::DeviceScan::InclusiveSum(cub, bytes, chunks, chunk_end, static_cast<int>(nd), stream));
         }
-        launch(del_scan, persistent_grid(), kMutWarps * 32, A.view(), A.desc, sorted, grp, chunk_end, m, firstpos);
+        {
+            // Chunks of a phase: at most one per 512 arena slots plus one per group.
+            const uint64_t need = A.seg_total * (kSegEdges / kDelChunk) + nd + 1;
+            if (need > chunk_map_cap) {
+                CK(cudaStreamSynchronize(stream));
+                dfree(chunk_map);
+                dmalloc(chunk_map, need);
+                chunk_map_cap = need;
+            }
+        }
+        launch(del_chunk_map, persistent_grid(), 256, grp, chunk_end, chunk_map);
+        const int ps = prof_begin(CIG_STAGE_DEL_SCAN);
+        launch(del_scan, sms * del_scan_blocks_per_sm(), kMutWarps * 32, A.view(), A.desc, sorted, grp, chunk_end,
+               chunk_map, m, firstpos, status->counters, forward ? seg_hot : nullptr);
+        prof_end(ps);
+        if (prof_on) prof[CIG_STAGE_DEL_SCAN].hits += nd;
         launch(del_apply, grid_for(nd), 256, A.view(), A.desc, sorted, m, firstpos, stats);
         launch(del_finish, persistent_grid(), 256, A.desc, sorted, grp, chunks, firstpos, compact, ccount, stats);
         // Ordered path: rows with repeated requests for a destination.
@@ -929,17 +1218,25 @@ struct cig_handle {
         uint32_t *gcount = small + (forward ? kGcF : kGcR);
         uint32_t *bcount = small + (forward ? kBigF : kBigR);
         int p = prof_begin(CIG_STAGE_GROUP);
-        if (forward || opt.algo == CIG_PR) {
-            launch(make_keys_add, grid_for(na), 256, d_au, d_av, m, n, kf, kr, status);
-            check_launch();
+        unsigned long long *sorted;
+        Groups grp;
+        if (presorted) {
+            sorted = forward ? t1 : t2;
+            grp = Groups{forward ? gaf : gar, forward ? gaendf : gaendr, small + (forward ? kGaF : kGaR)};
+        } else {
+            if (forward || opt.algo == CIG_PR) {
+                launch(make_keys_add, grid_for(na), 256, d_au, d_av, m, n, kf, kr, status);
+                check_launch();
+            }
+            sorted = sort_keys(keys, tmp, na);
+            grp = build_groups(sorted, na, groups, forward ? gendf : gendr, gcount);
         }
-        unsigned long long *sorted = sort_keys(keys, tmp, na);
         CK(cudaMemsetAsync(bcount, 0, sizeof(uint32_t), stream));
-        const Groups grp = build_groups(sorted, na, groups, forward ? gendf : gendr, gcount);
         prof_end(p);
         p = prof_begin(forward ? CIG_STAGE_ADD : CIG_STAGE_ADD_REV);
         launch(plan_add, persistent_grid(), 256, A.desc, sorted, grp, plan, A.alloc);
         launch(alloc_classes, 1, 64, A.alloc, status);
+        if (forward && refresh) launch(seg_assign_new, 1, 32, seg_table(), &A.alloc->seg_bump, status);
         unsigned long long *stats = with_stats ? status->counters : nullptr;
         const uint32_t *vals = forward ? d_av : d_au;
         launch(mutate_add, persistent_grid(), 256, A.view(), A.desc, sorted, grp, plan, A.alloc, vals, big, bcount,
@@ -965,7 +1262,7 @@ struct cig_handle {
         mutate_delete_arena(rev, d_du, d_dv, nd, false, false);
         p = prof_begin(CIG_STAGE_INVAL);
         launch_coop(inval_closure<A>, kTpb, fwd.view(), state, aff_stamp, epoch, list, small + kAff, n + 1,
-                    big_list(), n + 2, small + kAffTotal, status);
+                    big_list(), n + 2, small + kAffTotal, seg_hot, status);
         prof_end(p);
         p = prof_begin(CIG_STAGE_PULL);
         launch(reset_affected<A>, persistent_grid(), 256, list, small + kAffTotal, state);
@@ -1031,14 +1328,18 @@ struct cig_handle {
         stage_pairs(hu, hv, na, au, av, stage + 2 * bcap);
         dispatch([&](auto tag) { insert_phase_dev<decltype(tag)::value>(au, av, na); });
         CK(cudaEventRecord(ev[2], stream));
+        run_cache_service();
         CK(cudaEventRecord(ev[3], stream));
         finish();
         fill_stats(s, 0, na, false, true);
     }
 
+    // `mutation_after` (optional): an event the topology changes must wait
+    // for (a query wave still reading the rows); the key sort runs before it.
     void apply_batch(const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd, const uint32_t *d_au,
-                     const uint32_t *d_av, uint64_t na, cig_batch_stats *s) {
+                     const uint32_t *d_av, uint64_t na, cig_batch_stats *s, cudaEvent_t mutation_after = nullptr) {
         if (opt.algo == CIG_PR) {
+            if (mutation_after) CK(cudaStreamWaitEvent(stream, mutation_after, 0));
             if (pr64)
                 pr_batch<double>(d_du, d_dv, nd, d_au, d_av, na);
             else
@@ -1048,26 +1349,30 @@ struct cig_handle {
         } else {
             dispatch([&](auto tag) {
                 constexpr int A = decltype(tag)::value;
+                presort_batch(d_du, d_dv, nd, d_au, d_av, na);
+                if (mutation_after) CK(cudaStreamWaitEvent(stream, mutation_after, 0));
                 delete_phase_dev<A>(d_du, d_dv, nd);
                 CK(cudaEventRecord(ev[1], stream));
                 insert_phase_dev<A>(d_au, d_av, na);
                 CK(cudaEventRecord(ev[2], stream));
+                presorted = false;
             });
         }
+        run_cache_service();
         CK(cudaEventRecord(ev[3], stream));
         finish();
         fill_stats(s, nd, na, true, true);
     }
 
     void apply_batch_host(const uint32_t *hdu, const uint32_t *hdv, uint64_t nd, const uint32_t *hau,
-                          const uint32_t *hav, uint64_t na, cig_batch_stats *s) {
+                          const uint32_t *hav, uint64_t na, cig_batch_stats *s, cudaEvent_t mutation_after = nullptr) {
         require_ready();
         ensure_batch(std::max(nd, na));
         reset_counters();
         CK(cudaEventRecord(ev[0], stream));
         stage_pairs(hdu, hdv, nd, du, dv, stage);
         stage_pairs(hau, hav, na, au, av, stage + 2 * bcap);
-        apply_batch(du, dv, nd, au, av, na, s);
+        apply_batch(du, dv, nd, au, av, na, s, mutation_after);
     }
 
     void apply_batch_device(const uint32_t *ddu, const uint32_t *ddv, uint64_t nd, const uint32_t *dau,
@@ -1080,8 +1385,94 @@ struct cig_handle {
         apply_batch(ddu, ddv, nd, dau, dav, na, s);
     }
 
+    // The batched form: `count` batches (device arrays) queued back to back
+    // with one host synchronisation at the end.  Per batch the counters are
+    // snapshotted on the device and, if asked, the value digest is computed
+    // into a device slot, so every batch's result stays checkable.
+    std::vector<cudaEvent_t> bev;
+    unsigned long long *bsnap = nullptr, *bdig = nullptr;
+    uint32_t bsnap_cap = 0;
+
+    void apply_batches_device(const cig_update_batch *b, uint32_t count, cig_batch_stats *stats,
+                              uint64_t *digests) {
+        require_ready();
+        if (!b && count) throw CigError(CIG_ERR_ARG, "null batch list");
+        if (digests && opt.algo == CIG_PR) throw CigError(CIG_ERR_ARG, "PageRank has no integer digest");
+        uint64_t mx = 0;
+        for (uint32_t i = 0; i < count; ++i) {
+            if ((b[i].nd && (!b[i].del_u || !b[i].del_v)) || (b[i].na && (!b[i].add_u || !b[i].add_v)))
+                throw CigError(CIG_ERR_ARG, "null update array");
+            mx = std::max(mx, std::max(b[i].nd, b[i].na));
+        }
+        if (!count) return;
+        ensure_batch(mx);
+        if (count > bsnap_cap) {
+            CK(cudaStreamSynchronize(stream));
+            dfree(bsnap);
+            dfree(bdig);
+            dmalloc(bsnap, static_cast<size_t>(count) * 40);
+            dmalloc(bdig, count);
+            bsnap_cap = count;
+        }
+        while (bev.size() < 4ull * count) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            bev.push_back(e);
+        }
+        std::vector<uint64_t> launches(count);
+        for (uint32_t i = 0; i < count; ++i) {
+            const uint64_t l0 = n_launch;
+            reset_counters();
+            cudaEvent_t *e = bev.data() + 4ull * i;
+            CK(cudaEventRecord(e[0], stream));
+            if (opt.algo == CIG_PR) {
+                if (pr64)
+                    pr_batch<double>(b[i].del_u, b[i].del_v, b[i].nd, b[i].add_u, b[i].add_v, b[i].na);
+                else
+                    pr_batch<float>(b[i].del_u, b[i].del_v, b[i].nd, b[i].add_u, b[i].add_v, b[i].na);
+                CK(cudaEventRecord(e[1], stream));
+                CK(cudaEventRecord(e[2], stream));
+            } else {
+                dispatch([&](auto tag) {
+                    constexpr int A = decltype(tag)::value;
+                    presort_batch(b[i].del_u, b[i].del_v, b[i].nd, b[i].add_u, b[i].add_v, b[i].na);
+                    delete_phase_dev<A>(b[i].del_u, b[i].del_v, b[i].nd);
+                    CK(cudaEventRecord(e[1], stream));
+                    insert_phase_dev<A>(b[i].add_u, b[i].add_v, b[i].na);
+                    CK(cudaEventRecord(e[2], stream));
+                    presorted = false;
+                });
+            }
+            run_cache_service();
+            CK(cudaEventRecord(e[3], stream));
+            if (digests) {
+                CK(cudaMemsetAsync(bdig + i, 0, sizeof(unsigned long long), stream));
+                launch(value_digest, persistent_grid(), 256, state, n, bdig + i);
+            }
+            CK(cudaMemcpyAsync(bsnap + 40ull * i, status->counters, 40 * sizeof(unsigned long long),
+                               cudaMemcpyDeviceToDevice, stream));
+            check_launch();
+            launches[i] = n_launch - l0;
+        }
+        finish();
+        std::vector<unsigned long long> snap(40ull * count);
+        CK(cudaMemcpy(snap.data(), bsnap, snap.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+        if (digests) {
+            static_assert(sizeof(unsigned long long) == sizeof(uint64_t), "digest width");
+            CK(cudaMemcpy(digests, bdig, count * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+        }
+        for (uint32_t i = 0; i < count; ++i)
+            if (stats)
+                fill_stats_from(stats + i, snap.data() + 40ull * i, bev.data() + 4ull * i, launches[i], b[i].nd,
+                                b[i].na, true, true);
+    }
+
     void fill_stats(cig_batch_stats *s, uint64_t nd, uint64_t na, bool del, bool ins) {
-        const unsigned long long *c = h_status->counters;
+        fill_stats_from(s, h_status->counters, ev, n_launch - launch_mark, nd, na, del, ins);
+    }
+
+    void fill_stats_from(cig_batch_stats *s, const unsigned long long *c, const cudaEvent_t *evs, uint64_t launches,
+                         uint64_t nd, uint64_t na, bool del, bool ins) {
         if (!s) return;
         std::memset(s, 0, sizeof(*s));
         s->requested_deletes = nd;
@@ -1099,16 +1490,16 @@ struct cig_handle {
         s->cache_segments_loaded = c[kCntSegLoaded];
         s->cache_segments_evicted = c[kCntSegEvicted];
         s->pr_rounds = c[kCntPrRounds];
-        s->kernel_launches = n_launch - launch_mark;
+        s->kernel_launches = launches;
         float ms = 0;
         if (del) {
-            cudaEventElapsedTime(&ms, ev[0], ev[1]);
+            cudaEventElapsedTime(&ms, evs[0], evs[1]);
             s->ms_delete = ms;
         }
         if (ins) {
-            cudaEventElapsedTime(&ms, ev[1], ev[2]);
+            cudaEventElapsedTime(&ms, evs[1], evs[2]);
             s->ms_insert = ms;
-            cudaEventElapsedTime(&ms, ev[2], ev[3]);
+            cudaEventElapsedTime(&ms, evs[2], evs[3]);
             s->ms_cache = ms;
         }
         if (opt.algo == CIG_PR) {
@@ -1226,6 +1617,14 @@ struct cig_handle {
     // per-source form over the same kernels.
     void query_multi(int algo, const uint32_t *sources, uint32_t k, uint32_t width, uint32_t *out,
                      cig_query_stats *qs) {
+        const uint64_t launches0 = n_launch;
+        const uint32_t waves = query_launch(algo, sources, k, width, out);
+        query_finish(qs, waves, n_launch - launches0);
+    }
+
+    // Queue the waves of a query on qstream (after the updates already queued
+    // on the engine stream); q_ev[2] marks their end.  Returns the wave count.
+    uint32_t query_launch(int algo, const uint32_t *sources, uint32_t k, uint32_t width, uint32_t *out) {
         if (!loaded) throw CigError(CIG_ERR_ARG, "load a graph first");
         require_alive();
         if (algo != CIG_BFS && algo != CIG_SSSP) throw CigError(CIG_ERR_ARG, "queries are BFS or SSSP");
@@ -1238,7 +1637,6 @@ struct cig_handle {
         CK(cudaEventRecord(q_ev[0], stream));
         CK(cudaStreamWaitEvent(qstream, q_ev[0], 0));
         CK(cudaEventRecord(q_ev[1], qstream));
-        const uint64_t launches0 = n_launch;
         uint32_t waves = 0;
         for (uint32_t j0 = 0; j0 < k; j0 += width, ++waves) {
             const uint32_t kw = std::min(width, k - j0);
@@ -1250,13 +1648,16 @@ struct cig_handle {
             CK(cudaMemsetAsync(ms_small, 0, 8 * sizeof(uint32_t), qstream));
             CK(cudaMemcpyAsync(ms_src, sources + j0, kw * sizeof(uint32_t), cudaMemcpyHostToDevice, qstream));
             const MsFrontier fr{ms_q0, ms_q1, ms_small, ms_mask0, ms_mask1, n + 1};
-            const BigList bl{ms_big, ms_small + 3, kBigRowCap};
+            const BigList bl{ms_big, ms_small + 3, kBigRowCap, tune.split};
             ms_seed<<<1, kMsWidth, 0, qstream>>>(ms_src, kw, ms_dist, width, algo == CIG_BFS ? ms_visit : nullptr,
                                                  fr, qstatus);
             ++n_launch;
             if (algo == CIG_BFS)
                 launch_coop_on(qstream, ms_closure<kBfs>, kTpbMs, fwd.view(), ms_dist, width, ms_visit, fr, bl, n + 2,
                                qstatus);
+            else if (opt.flags & CIG_FLAG_WEIGHT_U255)
+                launch_coop_on(qstream, ms_closure<kSsspU>, kTpbMs, fwd.view(), ms_dist, width,
+                               static_cast<unsigned long long *>(nullptr), fr, bl, n + 2, qstatus);
             else
                 launch_coop_on(qstream, ms_closure<kSssp>, kTpbMs, fwd.view(), ms_dist, width,
                                static_cast<unsigned long long *>(nullptr), fr, bl, n + 2, qstatus);
@@ -1266,6 +1667,11 @@ struct cig_handle {
             check_launch();
         }
         CK(cudaEventRecord(q_ev[2], qstream));
+        return waves;
+    }
+
+    // Wait for the queued query, check its status, fill its stats.
+    void query_finish(cig_query_stats *qs, uint32_t waves, uint64_t launches) {
         CK(cudaStreamSynchronize(qstream));
         CK(cudaMemcpy(h_qstatus, qstatus, sizeof(Status), cudaMemcpyDeviceToHost));
         if (h_qstatus->err) {
@@ -1287,7 +1693,7 @@ struct cig_handle {
             qs->source_edges = h_qstatus->counters[kCntSrcEdges];
             qs->rounds = h_qstatus->counters[kCntRounds];
             qs->waves = waves;
-            qs->kernel_launches = n_launch - launches0;
+            qs->kernel_launches = launches;
         }
     }
 
@@ -1306,6 +1712,279 @@ struct cig_handle {
             query_multi(algo, sources + j0, kw, kMsWidth, ms_out, nullptr);
             CK(cudaMemcpy(out + static_cast<uint64_t>(j0) * n, ms_out, static_cast<uint64_t>(kw) * n * sizeof(uint32_t),
                           cudaMemcpyDeviceToHost));
+        }
+    }
+
+
+    // ------------------------------------------------------------ serving
+    struct ServeItem {
+        uint64_t ticket = 0;
+        cig_request r{};
+        std::vector<uint32_t> upd;  // du | dv | au | av of an update
+        double t_submit = 0;
+    };
+    struct Serve {
+        std::mutex mu;
+        std::condition_variable cv_work, cv_done, cv_space;
+        std::deque<ServeItem> queue;
+        std::unordered_map<uint64_t, cig_result> results;
+        std::unordered_set<uint64_t> open;  // submitted, result not yet taken
+        uint64_t next_ticket = 1;
+        uint64_t pending = 0;
+        bool stop = false;
+        std::thread worker;
+        cig_serve_options opt{};
+        std::chrono::steady_clock::time_point t0;
+        uint64_t chunk_cap = 0;  // largest update phase chunk the budget admits
+        uint32_t wave_cap = 64;  // sources per wave the budget admits
+        unsigned long long *digests = nullptr;  // device, one per wave slot
+        uint32_t *rows = nullptr;               // device wave_cap x n
+    };
+    std::unique_ptr<Serve> srv;
+    std::atomic<bool> serving{false};
+    // Device bytes per slot of the per-batch buffers that ensure_batch sizes.
+    static constexpr uint64_t kBytesPerBatchSlot = 384;
+
+    double serve_ms() const {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - srv->t0).count();
+    }
+
+    void serve_start(const cig_serve_options *o) {
+        require_ready();
+        if (serving) throw CigError(CIG_ERR_STATE, "already serving");
+        auto sv = std::make_unique<Serve>();
+        if (o) sv->opt = *o;
+        if (sv->opt.max_wave == 0 || sv->opt.max_wave > kMsWidth) sv->opt.max_wave = kMsWidth;
+        if (sv->opt.max_pending == 0) sv->opt.max_pending = 4096;
+        uint64_t budget = sv->opt.budget_bytes;
+        if (!budget) {
+            size_t fr = 0, tot = 0;
+            CK(cudaMemGetInfo(&fr, &tot));
+            budget = fr / 2;
+        }
+        // Half of the budget for update buffers, half for wave results.
+        sv->chunk_cap = std::max<uint64_t>(1024, std::min<uint64_t>(0x40000000ull, budget / 2 / kBytesPerBatchSlot));
+        const uint64_t rows = budget / 2 / (static_cast<uint64_t>(n) * sizeof(uint32_t));
+        sv->wave_cap = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(sv->opt.max_wave, rows)));
+        alloc_queries();
+        dmalloc(sv->digests, kMsWidth);
+        dmalloc(sv->rows, static_cast<size_t>(sv->wave_cap) * n);
+        sv->t0 = std::chrono::steady_clock::now();
+        srv = std::move(sv);
+        serving = true;
+        srv->worker = std::thread([this] { serve_loop(); });
+    }
+
+    void serve_stop() {
+        if (!srv) return;
+        {
+            std::lock_guard<std::mutex> lk(srv->mu);
+            srv->stop = true;
+        }
+        srv->cv_work.notify_all();
+        if (srv->worker.joinable()) srv->worker.join();
+        dfree(srv->digests);
+        dfree(srv->rows);
+        srv.reset();
+        serving = false;
+    }
+
+    uint64_t serve_submit(const cig_request *r) {
+        if (!srv) throw CigError(CIG_ERR_STATE, "not serving");
+        if (!r) throw CigError(CIG_ERR_ARG, "null request");
+        ServeItem it;
+        it.r = *r;
+        if (r->kind == CIG_REQ_UPDATE) {
+            if ((r->nd && (!r->del_u || !r->del_v)) || (r->na && (!r->add_u || !r->add_v)))
+                throw CigError(CIG_ERR_ARG, "null update array");
+            it.upd.resize(2 * (r->nd + r->na));
+            if (r->nd) {
+                std::memcpy(it.upd.data(), r->del_u, r->nd * sizeof(uint32_t));
+                std::memcpy(it.upd.data() + r->nd, r->del_v, r->nd * sizeof(uint32_t));
+            }
+            if (r->na) {
+                std::memcpy(it.upd.data() + 2 * r->nd, r->add_u, r->na * sizeof(uint32_t));
+                std::memcpy(it.upd.data() + 2 * r->nd + r->na, r->add_v, r->na * sizeof(uint32_t));
+            }
+        } else if (r->kind == CIG_REQ_BFS || r->kind == CIG_REQ_SSSP) {
+            if (r->source >= n) throw CigError(CIG_ERR_ARG, "query source out of range");
+        } else {
+            throw CigError(CIG_ERR_ARG, "unknown request kind");
+        }
+        std::unique_lock<std::mutex> lk(srv->mu);
+        srv->cv_space.wait(lk, [&] { return srv->pending < srv->opt.max_pending || srv->stop; });
+        if (srv->stop) throw CigError(CIG_ERR_STATE, "serving is stopping");
+        it.ticket = srv->next_ticket++;
+        it.t_submit = serve_ms();
+        const uint64_t t = it.ticket;
+        srv->open.insert(t);
+        srv->queue.push_back(std::move(it));
+        ++srv->pending;
+        lk.unlock();
+        srv->cv_work.notify_one();
+        return t;
+    }
+
+    bool serve_take(uint64_t ticket, cig_result *res, bool block) {
+        if (!srv) throw CigError(CIG_ERR_STATE, "not serving");
+        std::unique_lock<std::mutex> lk(srv->mu);
+        if (!srv->open.count(ticket)) throw CigError(CIG_ERR_ARG, "unknown ticket or result already taken");
+        auto ready = [&] { return srv->results.count(ticket) != 0; };
+        if (block)
+            srv->cv_done.wait(lk, ready);
+        else if (!ready())
+            return false;
+        if (res) *res = srv->results[ticket];
+        srv->results.erase(ticket);
+        srv->open.erase(ticket);
+        return true;
+    }
+
+    void serve_publish(const ServeItem &it, const cig_result &r) {
+        {
+            std::lock_guard<std::mutex> lk(srv->mu);
+            srv->results[it.ticket] = r;
+            --srv->pending;
+        }
+        srv->cv_done.notify_all();
+        srv->cv_space.notify_all();
+    }
+
+    static int32_t error_code(const std::exception &e) {
+        if (const auto *c = dynamic_cast<const CigError *>(&e)) return c->code;
+        return CIG_ERR_DEVICE;
+    }
+
+    // One update request: whole, or (over the admitted size) as deletion
+    // chunks followed by insertion chunks, which leave the same rows and
+    // values.  `after`: event of a wave the mutation must wait for.
+    void serve_update(const ServeItem &it, cig_result &res, cudaEvent_t after) {
+        const uint64_t nd = it.r.nd, na = it.r.na, cap = srv->chunk_cap;
+        const uint32_t *d_u = it.upd.data(), *d_v = d_u + nd, *a_u = d_u + 2 * nd, *a_v = a_u + na;
+        if (nd <= cap && na <= cap) {
+            apply_batch_host(d_u, d_v, nd, a_u, a_v, na, nullptr, after);
+        } else {
+            for (uint64_t o = 0; o < nd; o += cap, after = nullptr)
+                apply_batch_host(d_u + o, d_v + o, std::min(cap, nd - o), nullptr, nullptr, 0, nullptr, after);
+            for (uint64_t o = 0; o < na; o += cap, after = nullptr)
+                apply_batch_host(nullptr, nullptr, 0, a_u + o, a_v + o, std::min(cap, na - o), nullptr, after);
+        }
+        res.digest = opt.algo == CIG_PR ? 0 : digest();
+    }
+
+    void serve_loop() {
+        cudaSetDevice(device);
+        for (;;) {
+            std::vector<ServeItem> wave;
+            ServeItem upd;
+            bool have_upd = false;
+            {
+                std::unique_lock<std::mutex> lk(srv->mu);
+                srv->cv_work.wait(lk, [&] { return srv->stop || !srv->queue.empty(); });
+                if (srv->queue.empty()) return;
+                if (srv->queue.front().r.kind == CIG_REQ_UPDATE) {
+                    upd = std::move(srv->queue.front());
+                    srv->queue.pop_front();
+                    have_upd = true;
+                } else {
+                    // Queries do not change the graph, so the wave takes every
+                    // query of the front one's kind up to the next update.
+                    const int32_t kind = srv->queue.front().r.kind;
+                    for (auto it = srv->queue.begin(); it != srv->queue.end() && wave.size() < srv->wave_cap;) {
+                        if (it->r.kind == CIG_REQ_UPDATE) break;
+                        if (it->r.kind == kind) {
+                            wave.push_back(std::move(*it));
+                            it = srv->queue.erase(it);
+                        } else {
+                            ++it;
+                        }
+                    }
+                    // The update right behind a wave starts beside it.
+                    if (!srv->queue.empty() && srv->queue.front().r.kind == CIG_REQ_UPDATE) {
+                        upd = std::move(srv->queue.front());
+                        srv->queue.pop_front();
+                        have_upd = true;
+                    }
+                }
+            }
+            if (!wave.empty()) serve_wave(wave, have_upd ? &upd : nullptr);
+            else if (have_upd) {
+                cig_result res{};
+                res.submit_ms = upd.t_submit;
+                res.start_ms = serve_ms();
+                try {
+                    serve_update(upd, res, nullptr);
+                    res.status = CIG_OK;
+                } catch (const std::exception &e) {
+                    res.status = error_code(e);
+                }
+                res.done_ms = serve_ms();
+                serve_publish(upd, res);
+            }
+        }
+    }
+
+    // A wave of queries of one kind (one bitmask wave), and optionally the
+    // update queued right behind it: its copy and key sort overlap the wave,
+    // its topology changes wait for the wave.
+    void serve_wave(std::vector<ServeItem> &wave, ServeItem *upd) {
+        const uint32_t k = static_cast<uint32_t>(wave.size());
+        const int algo = wave[0].r.kind == CIG_REQ_BFS ? CIG_BFS : CIG_SSSP;
+        std::vector<uint32_t> src(k);
+        for (uint32_t j = 0; j < k; ++j) src[j] = wave[j].r.source;
+        const double t_start = serve_ms();
+        int32_t status = CIG_OK;
+        std::vector<unsigned long long> dig(k, 0);
+        bool launched = false;
+        try {
+            query_launch(algo, src.data(), k, k, srv->rows);
+            CK(cudaMemsetAsync(srv->digests, 0, k * sizeof(unsigned long long), qstream));
+            ms_row_digest<<<dim3(static_cast<unsigned>(std::min<uint64_t>(sms * 2, (n + 255) / 256)), k), 256, 0,
+                            qstream>>>(srv->rows, n, srv->digests);
+            ++n_launch;
+            check_launch();
+            CK(cudaEventRecord(q_ev[2], qstream));
+            launched = true;
+        } catch (const std::exception &e) {
+            status = error_code(e);
+        }
+        cig_result ures{};
+        if (upd) {
+            ures.submit_ms = upd->t_submit;
+            ures.start_ms = serve_ms();
+            try {
+                serve_update(*upd, ures, launched ? q_ev[2] : nullptr);
+                ures.status = CIG_OK;
+            } catch (const std::exception &e) {
+                ures.status = error_code(e);
+            }
+        }
+        if (launched) {
+            try {
+                query_finish(nullptr, 1, 0);
+                CK(cudaMemcpy(dig.data(), srv->digests, k * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+                for (uint32_t j = 0; j < k; ++j)
+                    if (wave[j].r.out)
+                        CK(cudaMemcpy(wave[j].r.out, srv->rows + static_cast<uint64_t>(j) * n, n * sizeof(uint32_t),
+                                      cudaMemcpyDeviceToHost));
+            } catch (const std::exception &e) {
+                status = error_code(e);
+            }
+        }
+        const double t_done = serve_ms();
+        for (uint32_t j = 0; j < k; ++j) {
+            cig_result r{};
+            r.status = status;
+            r.wave = k;
+            r.digest = dig[j];
+            r.submit_ms = wave[j].t_submit;
+            r.start_ms = t_start;
+            r.done_ms = t_done;
+            serve_publish(wave[j], r);
+        }
+        if (upd) {
+            ures.done_ms = serve_ms();
+            serve_publish(*upd, ures);
         }
     }
 
@@ -1341,21 +2020,27 @@ void cig_set_unbound_error(const std::string &message) { g_create_error = messag
 namespace {
 
 template <class F>
-int guarded(cig_handle *h, F f) {
+int guarded(cig_handle *h, F f, bool while_serving = false) {
     if (!h) return CIG_ERR_ARG;
+    if (h->serving && !while_serving) {
+        h->err = "the handle is serving requests (cig_serve_stop first)";
+        return CIG_ERR_STATE;
+    }
     try {
         CK(cudaSetDevice(h->device));
         f();
         return CIG_OK;
     } catch (const CigError &e) {
-        h->err = e.what();
+        // Serving calls may come from several threads: their errors go to
+        // the calling thread's cig_last_error(NULL) text.
+        (while_serving ? g_create_error : h->err) = e.what();
         if (e.code == CIG_ERR_DEVICE) h->dead = true;
         return e.code;
     } catch (const std::bad_alloc &) {
-        h->err = "host allocation failed";
+        (while_serving ? g_create_error : h->err) = "host allocation failed";
         return CIG_ERR_NOMEM;
     } catch (const std::exception &e) {
-        h->err = e.what();
+        (while_serving ? g_create_error : h->err) = e.what();
         return CIG_ERR_DEVICE;
     }
 }
@@ -1401,6 +2086,7 @@ int cig_create(const cig_options *o, cig_handle **out) {
 
 int cig_destroy(cig_handle *h) {
     if (!h) return CIG_ERR_ARG;
+    h->serve_stop();
     h->destroy();
     delete h;
     return CIG_OK;
@@ -1552,7 +2238,14 @@ int cig_graph_info_get(cig_handle *h, cig_graph_info *info) {
         info->arena_used_edges = std::min<uint64_t>(al.seg_bump, h->fwd.seg_total) * kSegEdges;
         info->segment_edges = kSegEdges;
         info->segments_total = h->fwd.seg_total;
-        info->segments_resident = std::min<uint64_t>(h->resident, std::min<uint64_t>(al.seg_bump, h->fwd.seg_total));
+        {
+            std::vector<int32_t> slot(h->fwd.seg_total);
+            CK(cudaMemcpy(slot.data(), h->fwd.seg_slot, slot.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
+            const uint64_t used = std::min<uint64_t>(al.seg_bump, h->fwd.seg_total);
+            uint64_t r = 0;
+            for (uint64_t s = 0; s < used; ++s) r += slot[s] >= 0;
+            info->segments_resident = r;
+        }
         info->cache_capacity_segments = h->cache_slots;
         size_t free_b = 0, total_b = 0;
         cudaMemGetInfo(&free_b, &total_b);
@@ -1576,6 +2269,45 @@ int cig_profile_read(cig_handle *h, cig_stage_profile *out, uint32_t count) {
         if (!out) throw CigError(CIG_ERR_ARG, "null output");
         std::memcpy(out, h->prof, std::min<uint32_t>(count, CIG_STAGE_COUNT) * sizeof(cig_stage_profile));
     });
+}
+
+int cig_autotune(cig_handle *h, cig_tune_result *res) {
+    return guarded(h, [&] { h->autotune(res); });
+}
+
+int cig_serve_start(cig_handle *h, const cig_serve_options *o) {
+    return guarded(h, [&] { h->serve_start(o); });
+}
+
+int cig_serve_submit(cig_handle *h, const cig_request *r, uint64_t *ticket) {
+    return guarded(
+        h, [&] {
+            if (!ticket) throw CigError(CIG_ERR_ARG, "null ticket");
+            *ticket = h->serve_submit(r);
+        },
+        true);
+}
+
+int cig_serve_wait(cig_handle *h, uint64_t ticket, cig_result *res) {
+    return guarded(h, [&] { h->serve_take(ticket, res, true); }, true);
+}
+
+int cig_serve_poll(cig_handle *h, uint64_t ticket, cig_result *res, int *done) {
+    return guarded(
+        h, [&] {
+            if (!done) throw CigError(CIG_ERR_ARG, "null done flag");
+            *done = h->serve_take(ticket, res, false) ? 1 : 0;
+        },
+        true);
+}
+
+int cig_serve_stop(cig_handle *h) {
+    return guarded(h, [&] { h->serve_stop(); }, true);
+}
+
+int cig_apply_batches_device(cig_handle *h, const cig_update_batch *batches, uint32_t count, cig_batch_stats *stats,
+                             uint64_t *digests) {
+    return guarded(h, [&] { h->apply_batches_device(batches, count, stats, digests); });
 }
 
 int cig_query_bfs_multi(cig_handle *h, const uint32_t *sources, uint32_t k, uint32_t *out_depth) {

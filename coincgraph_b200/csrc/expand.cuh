@@ -52,7 +52,7 @@ __device__ __forceinline__ void flush_counters(Status *st, const ExpandCounters 
     warp_count(&st->counters[group + 3], c.hits);
 }
 
-// Rows with at least kSplitDeg entries are not expanded by the block that
+// Rows with at least `split` entries (default kSplitDeg) are not expanded by the block that
 // holds them: they are appended to a list that every block of the grid
 // then expands in kSplitChunk-entry chunks (expand_deferred), so that one
 // hub row does not serialise a whole round on one block.
@@ -69,6 +69,7 @@ struct Defer {
     BigRow *rows;     // null: expand every row in place
     uint32_t *count;
     uint32_t cap;
+    uint32_t split;   // rows of at least this many entries are deferred
 };
 
 // Op must provide: __device__ bool edge(bool valid, uint32_t x, P payload, uint32_t y) const;
@@ -77,7 +78,7 @@ struct Defer {
 template <int TPB, class Op, class P>
 __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint32_t x, P payload,
                                             uint64_t off, uint32_t deg, const Op &op, ExpandSmem<TPB, P> &sm,
-                                            ExpandCounters &cnt, const Defer &defer = Defer{nullptr, nullptr, 0}) {
+                                            ExpandCounters &cnt, const Defer &defer = Defer{nullptr, nullptr, 0, 0}) {
     const uint32_t lane = lane_id();
     const uint32_t warp = threadIdx.x >> 5;
     if (has) {
@@ -85,7 +86,7 @@ __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint3
         cnt.edges += deg;
         if (view.cached(off)) cnt.edges_cached += deg;
     }
-    if (has && defer.rows && deg >= kSplitDeg) {
+    if (has && defer.rows && deg >= defer.split) {
         const uint32_t i = atomicAdd(defer.count, 1u);
         if (i < defer.cap) {
             defer.rows[i] = BigRow{off, static_cast<unsigned long long>(payload), x, deg};

@@ -24,6 +24,7 @@
 //   - grouping, matching, allocation and appends all run on the GPU.
 #pragma once
 
+#include <cub/block/block_radix_sort.cuh>
 #include <cub/block/block_scan.cuh>
 
 #include "common.cuh"
@@ -126,6 +127,123 @@ __global__ void group_scatter(const unsigned long long *keys, uint32_t m, const 
     if (i + 1 == m || keys[i + 1] == kKeyNone) {  // last valid key closes the last group
         end[pos[i] + flags[i] - 1] = i + 1;
         *count = pos[i] + flags[i];
+    }
+}
+
+// ---------------------------------------------------------------- one sort per batch
+// The four key sets of a whole batch (forward and reverse deletion keys,
+// forward and reverse addition keys) are packed into one array and sorted
+// by one radix sort: key = set << 2F | first << F | second with F bits per
+// field (2^F > n and > the phase sizes), so the sort has 2 + 2F significant
+// bits instead of four sorts of 32 + log2(n) bits.  An invalid record gets
+// all-ones fields and sorts to the end of its set.  Sets occupy [0, nd),
+// [nd, 2nd), [2nd, 2nd+na), [2nd+na, 2nd+2na).
+struct PackedSets {
+    uint32_t off[5];
+    uint32_t f;  // field width F
+};
+
+__global__ void make_keys_batch(const uint32_t *du, const uint32_t *dv, uint32_t nd, const uint32_t *au,
+                                const uint32_t *av, uint32_t na, uint32_t n, PackedSets ps,
+                                unsigned long long *out, Status *st) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t total = ps.off[4];
+    if (i >= total) return;
+    const uint32_t f = ps.f;
+    const unsigned long long none = (1ull << f) - 1;
+    uint32_t set, first, second;
+    bool ok;
+    if (i < ps.off[2]) {
+        set = i < ps.off[1] ? 0u : 1u;
+        const uint32_t j = i - ps.off[set];
+        const uint32_t u = du[j], v = dv[j];
+        ok = u < n && v < n;
+        first = set == 0 ? u : v;
+        second = set == 0 ? v : u;
+    } else {
+        set = i < ps.off[3] ? 2u : 3u;
+        const uint32_t j = i - ps.off[set];
+        const uint32_t u = au[j], v = av[j];
+        ok = u < n && v < n;
+        first = set == 2 ? u : v;
+        second = j;
+        if (!ok && set == 2) atomicAdd(&st->counters[kCntInvalid], 1ull);
+    }
+    const unsigned long long a = ok ? first : none, b = ok ? second : none;
+    out[i] = (static_cast<unsigned long long>(set) << (2 * f)) | (a << f) | b;
+}
+
+// Small batches (at most kSmallSortKeys packed keys): one block sorts them
+// in shared memory, instead of a device-wide radix sort whose passes are
+// each a few microseconds of launch and latency.
+constexpr int kSmallSortThreads = 256;
+constexpr int kSmallSortItems = 16;
+constexpr uint32_t kSmallSortKeys = kSmallSortThreads * kSmallSortItems;
+
+__global__ void __launch_bounds__(kSmallSortThreads)
+    sort_small(const unsigned long long *in, uint32_t total, int end_bit, unsigned long long *out) {
+    using Sort = cub::BlockRadixSort<unsigned long long, kSmallSortThreads, kSmallSortItems>;
+    __shared__ typename Sort::TempStorage tmp;
+    unsigned long long k[kSmallSortItems];
+#pragma unroll
+    for (int j = 0; j < kSmallSortItems; ++j) {
+        const uint32_t i = threadIdx.x * kSmallSortItems + j;
+        k[j] = i < total ? in[i] : ~0ull;
+    }
+    Sort(tmp).Sort(k, 0, end_bit);
+#pragma unroll
+    for (int j = 0; j < kSmallSortItems; ++j) {
+        const uint32_t i = threadIdx.x * kSmallSortItems + j;
+        if (i < total) out[i] = k[j];
+    }
+}
+
+// Sorted packed keys -> the usual (first << 32 | second) keys of each set,
+// and group flags (first key of every source run inside its set).
+__global__ void unpack_keys_batch(const unsigned long long *sorted, PackedSets ps, unsigned long long *k0,
+                                  unsigned long long *k1, unsigned long long *k2, unsigned long long *k3,
+                                  uint32_t *flags) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ps.off[4]) return;
+    const uint32_t f = ps.f;
+    const unsigned long long mask = (1ull << f) - 1;
+    const unsigned long long k = sorted[i];
+    const uint32_t set = static_cast<uint32_t>(k >> (2 * f)) & 3u;  // & 3: a small-sort pad (~0) reads as set 3
+    const unsigned long long a = (k >> f) & mask, b = k & mask;
+    const bool ok = a != mask;
+    unsigned long long *dst = set == 0 ? k0 : set == 1 ? k1 : set == 2 ? k2 : k3;
+    dst[i - ps.off[set]] = ok ? ((a << kKeyShift) | b) : kKeyNone;
+    flags[i] = (ok && (i == ps.off[set] || (sorted[i - 1] >> f) != (k >> f))) ? 1u : 0u;
+}
+
+// Groups of the four sets from one exclusive scan of the flags; group
+// indices and key positions are relative to the set.
+struct SetGroups {
+    uint32_t *start[4];
+    uint32_t *end[4];
+    uint32_t *count[4];
+};
+
+__global__ void group_scatter_batch(const unsigned long long *sorted, PackedSets ps, const uint32_t *flags,
+                                    const uint32_t *pos, SetGroups sg) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ps.off[4]) return;
+    const uint32_t f = ps.f;
+    const unsigned long long mask = (1ull << f) - 1;
+    const unsigned long long k = sorted[i];
+    if (((k >> f) & mask) == mask) return;  // invalid record
+    const uint32_t set = static_cast<uint32_t>(k >> (2 * f)) & 3u;  // & 3: a small-sort pad (~0) reads as set 3
+    const uint32_t s0 = ps.off[set], s1 = ps.off[set + 1];
+    const uint32_t base = pos[s0];
+    const uint32_t local = i - s0;
+    const uint32_t g = pos[i] - base;
+    if (flags[i]) {
+        sg.start[set][g] = local;
+        if (g > 0) sg.end[set][g - 1] = local;
+    }
+    if (i + 1 == s1 || ((sorted[i + 1] >> f) & mask) == mask) {  // last valid key of the set
+        sg.end[set][g + flags[i] - 1] = local + 1;
+        *sg.count[set] = g + flags[i];
     }
 }
 
@@ -476,76 +594,145 @@ __global__ void del_classify(const RowDesc *desc, const unsigned long long *keys
     }
 }
 
-// Warps take contiguous ranges of 512-entry chunks (uniform work), find the
-// group of their first chunk by one binary search and then advance through
-// the groups in order; each chunk records the first live match of every key.
+// Chunk runs are dealt round-robin to the warps: run r (kDelRun consecutive
+// 512-entry chunks) goes to warp r mod warps, so the chunks of one long row
+// spread over the whole grid while a warp still reuses a row's keys for a
+// few chunks.  `chunk_map[c]` is the group of chunk c (del_chunk_map);
 // `chunk_end` is the inclusive prefix sum of `chunks` over scan_n entries.
+// Each chunk records the first live match of every key (atomicMin).
+//
+// Membership test per row entry, by the row's number of requests: up to
+// kDelLaneKeys, compare against the keys held in lanes (about 9 instructions
+// per request per 4 entries); up to kDelCmpKeys, a 64-bit filter in a
+// register (6-bit hash) and a linear check of the keys in shared memory on a
+// filter hit; beyond, a per-warp bit filter in shared memory (32 bits per
+// request rounded up to a power of two, 1024..16384 bits) and a binary search
+// on a hit.  Filters are built once per group, so most entries are rejected
+// by one test and only filter hits pay the exact search.
+constexpr uint32_t kDelLaneKeys = 2;  // up to this many requests: compare against lane registers
+constexpr uint32_t kDelCmpKeys = 8;   // up to this many: 64-bit register filter, else the shared-memory filter
+constexpr uint32_t kDelFilterWords = 512;
+
+__device__ __forceinline__ uint32_t del_hash(uint32_t y, uint32_t shift) { return (y * 2654435761u) >> shift; }
+
+constexpr uint32_t kDelRun = 4;
+
+// chunk_map[c] = group of chunk c; one warp per group, lanes over its chunks.
+__global__ void del_chunk_map(Groups gr, const uint32_t *chunk_end, uint32_t *chunk_map) {
+    const uint32_t ng = *gr.count;
+    const uint32_t lane = lane_id();
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ng; g += warps) {
+        const uint32_t c0 = g ? chunk_end[g - 1] : 0u, c1 = chunk_end[g];
+        for (uint32_t c = c0 + lane; c < c1; c += 32u) chunk_map[c] = g;
+    }
+}
+
 __global__ void __launch_bounds__(kMutWarps * 32)
     del_scan(AdjView view, const RowDesc *desc, const unsigned long long *keys, Groups gr, const uint32_t *chunk_end,
-             uint32_t scan_n, uint32_t *firstpos) {
+             const uint32_t *chunk_map, uint32_t scan_n, uint32_t *firstpos, unsigned long long *stats,
+             uint32_t *seg_hot) {
     __shared__ uint32_t skeys[kMutWarps][kSmemKeys];
+    __shared__ uint32_t sfilt[kMutWarps][kDelFilterWords];
     uint32_t *sk = skeys[threadIdx.x >> 5];
+    uint32_t *filt = sfilt[threadIdx.x >> 5];
     const uint32_t lane = lane_id();
-    const uint32_t ng = *gr.count;
     const uint32_t total = scan_n ? chunk_end[scan_n - 1] : 0u;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t per = (total + warps - 1) / warps;
-    const uint32_t c_begin = min(total, wid * per), c_end = min(total, c_begin + per);
-    uint32_t g = 0;
-    {
-        uint32_t lo = 0, hi = ng;  // first group whose inclusive end exceeds c_begin
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (chunk_end[mid] > c_begin)
-                hi = mid;
-            else
-                lo = mid + 1;
+    uint32_t g_ready = ~0u;  // group whose keys are loaded in kd / filt / sk
+    uint32_t gs = 0, ge = 0, nk = 0, kd = 0, fshift = 18;
+    unsigned long long rfilt = 0;
+    RowDesc d{};
+    unsigned long long uhi = 0;
+    uint32_t scanned = 0, scanned_cached = 0;
+    for (uint32_t c = wid * kDelRun; c < total; c += (c % kDelRun == kDelRun - 1) ? (warps - 1) * kDelRun + 1 : 1) {
+        const uint32_t g = chunk_map[c];
+        if (g != g_ready) {
+            __syncwarp();
+            g_ready = g;
+            gs = gr.start[g];
+            ge = gr.end[g];
+            nk = ge - gs;
+            const uint32_t u = key_src(keys[gs]);
+            d = desc[u];
+            uhi = static_cast<unsigned long long>(u) << kKeyShift;
+            kd = lane < nk ? key_low(keys[gs + lane]) : 0u;
+            if (nk > kDelLaneKeys && nk <= kDelCmpKeys) {
+                // 64-bit register filter (6-bit hash) + the keys in shared memory
+                const unsigned long long bit = lane < nk ? 1ull << del_hash(kd, 26) : 0ull;
+                const uint32_t lo = __reduce_or_sync(kFull, static_cast<uint32_t>(bit));
+                const uint32_t hi = __reduce_or_sync(kFull, static_cast<uint32_t>(bit >> 32));
+                rfilt = (static_cast<unsigned long long>(hi) << 32) | lo;
+                if (lane < nk) sk[lane] = kd;
+            }
+            if (nk > kDelCmpKeys) {
+                // words = nk rounded up to a power of two in [32, 512]
+                const uint32_t words = min(kDelFilterWords, max(32u, 1u << (32 - __clz(nk - 1))));
+                fshift = 32u - (5u + (31u - __clz(words)));  // hash -> log2(32 * words) bits
+                for (uint32_t j = lane; j < words; j += 32u) filt[j] = 0u;
+                __syncwarp();
+                for (uint32_t j = lane; j < nk; j += 32u) {
+                    const uint32_t y = key_low(keys[gs + j]);
+                    const uint32_t h = del_hash(y, fshift);
+                    atomicOr(filt + (h >> 5), 1u << (h & 31u));
+                    if (nk <= kSmemKeys) sk[j] = y;
+                }
+            }
+            __syncwarp();
         }
-        g = lo;
-    }
-    for (uint32_t c = c_begin; c < c_end; ++c) {
-        while (chunk_end[g] <= c) ++g;
         const uint32_t k0 = (c - (g ? chunk_end[g - 1] : 0u)) * kDelChunk;
-        const uint32_t gs = gr.start[g];
-        const uint32_t ge = gr.end[g];
-        const uint32_t nk = ge - gs;
-        const uint32_t u = key_src(keys[gs]);
-        const RowDesc d = desc[u];
-        const unsigned long long uhi = static_cast<unsigned long long>(u) << kKeyShift;
-        const uint32_t kd = lane < nk ? key_low(keys[gs + lane]) : 0u;
-        if (nk > 32u && nk <= kSmemKeys) {
-            for (uint32_t j = lane; j < nk; j += 32u) sk[j] = key_low(keys[gs + j]);
-        }
-        __syncwarp();
         // A 512-entry chunk never straddles a segment (segments hold 2^14).
         const uint32_t *src = view.at(d.off + k0);
+        const uint32_t len_here = min(kDelChunk, d.len - k0);
+        scanned += len_here;
+        if (view.cached(d.off + k0)) scanned_cached += len_here;
+        if (seg_hot && lane == 0) atomicAdd(seg_hot + ((d.off + k0) >> kSegShift), len_here);
+        // Short rows (most groups) end after one or two 128-entry steps.
+        const uint32_t steps = (len_here + 127u) / 128u;
+        uint4 q[kDelChunk / 128u];
 #pragma unroll
         for (uint32_t s = 0; s < kDelChunk / 128u; ++s) {
             const uint32_t kk = k0 + 128u * s + 4u * lane;
-            uint32_t e[4] = {kTomb, kTomb, kTomb, kTomb};
-            if (kk < d.len) {
-                const uint4 q = *reinterpret_cast<const uint4 *>(src + 128u * s + 4u * lane);
-                e[0] = q.x;
-                e[1] = q.y;
-                e[2] = q.z;
-                e[3] = q.w;
+            q[s] = (s < steps && kk < d.len) ? *reinterpret_cast<const uint4 *>(src + 128u * s + 4u * lane)
+                                             : make_uint4(kTomb, kTomb, kTomb, kTomb);
+        }
 #pragma unroll
-                for (int t = 0; t < 4; ++t)
-                    if (kk + t >= d.len) e[t] = kTomb;
-            }
-            int hit[4] = {-1, -1, -1, -1};
-            if (nk <= 32u) {
+        for (uint32_t s = 0; s < kDelChunk / 128u; ++s) {
+            if (s >= steps) continue;  // warp-uniform; keeps the loop unrolled (q[] in registers)
+            const uint32_t kk = k0 + 128u * s + 4u * lane;
+            uint32_t e[4] = {q[s].x, q[s].y, q[s].z, q[s].w};
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+                if (kk + t >= d.len) e[t] = kTomb;
+            if (nk > kDelLaneKeys && nk <= kDelCmpKeys) {
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    if (e[t] == kTomb || !((rfilt >> del_hash(e[t], 26)) & 1ull)) continue;
+                    for (uint32_t j = 0; j < nk; ++j)
+                        if (sk[j] == e[t]) {
+                            atomicMin(firstpos + gs + j, kk + t);
+                            break;
+                        }
+                }
+            } else if (nk <= kDelCmpKeys) {
+                int hit[4] = {-1, -1, -1, -1};
                 for (uint32_t j = 0; j < nk; ++j) {
                     const uint32_t kj = __shfl_sync(kFull, kd, j);
 #pragma unroll
                     for (int t = 0; t < 4; ++t)
                         if (e[t] == kj) hit[t] = static_cast<int>(j);
                 }
+#pragma unroll
+                for (int t = 0; t < 4; ++t)
+                    if (hit[t] >= 0 && e[t] != kTomb) atomicMin(firstpos + gs + hit[t], kk + t);
             } else {
 #pragma unroll
                 for (int t = 0; t < 4; ++t) {
                     if (e[t] == kTomb) continue;
+                    const uint32_t h = del_hash(e[t], fshift);
+                    if (!((filt[h >> 5] >> (h & 31u)) & 1u)) continue;
+                    int hit = -1;
                     if (nk <= kSmemKeys) {
                         uint32_t a = 0, b = nk;
                         while (a < b) {
@@ -555,18 +742,21 @@ __global__ void __launch_bounds__(kMutWarps * 32)
                             else
                                 b = mid;
                         }
-                        if (a < nk && sk[a] == e[t]) hit[t] = static_cast<int>(a);
+                        if (a < nk && sk[a] == e[t]) hit = static_cast<int>(a);
                     } else {
                         uint32_t run, req;
-                        if (find_run(keys, gs, ge, uhi | e[t], run, req)) hit[t] = static_cast<int>(run - gs);
+                        if (find_run(keys, gs, ge, uhi | e[t], run, req)) hit = static_cast<int>(run - gs);
                     }
+                    if (hit >= 0) atomicMin(firstpos + gs + hit, kk + t);
                 }
             }
-#pragma unroll
-            for (int t = 0; t < 4; ++t)
-                if (hit[t] >= 0 && e[t] != kTomb) atomicMin(firstpos + gs + hit[t], kk + t);
         }
-        __syncwarp();
+    }
+    if (stats) {
+        // lane 0 of every warp holds the warp's totals (all lanes counted the same chunks)
+        if (lane == 0 && scanned) atomicAdd(&stats[kCntDelScanned], static_cast<unsigned long long>(scanned));
+        if (lane == 0 && scanned_cached)
+            atomicAdd(&stats[kCntDelScannedCached], static_cast<unsigned long long>(scanned_cached));
     }
 }
 

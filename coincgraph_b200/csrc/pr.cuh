@@ -12,6 +12,15 @@
 // rounds with grid barriers (no host count read per round); the rank is
 // FP32 with a per-vertex Kahan compensation term (or FP64 throughout); the
 // batch reports the FP64 L1 norm of the residual.
+//
+// FP32 residuals lose precision where many contributions pile up between two
+// consumptions: a vertex with in-degree k takes up to k atomic adds per round,
+// and the rounding of each (half an ulp of the running sum) adds up to about
+// 6e-8 * sqrt(k) of its residual.  So in FP32 mode vertices whose in-degree
+// was at least kPrHubInDeg at load keep their residual in an FP64 slot;
+// everything else stays FP32.  The hub set is a bitmap (n/8 bytes) with a
+// per-word prefix count (slot = prefix + rank in the word), small enough to
+// stay in L2, since every scattered edge looks its destination up.
 #pragma once
 
 #include "common.cuh"
@@ -22,10 +31,15 @@ namespace cig {
 constexpr float kAlphaF = 0.85f;
 constexpr double kAlphaD = 0.85;
 
+constexpr uint32_t kPrHubInDeg = 256;
+
 template <class T>
 struct PrArrays {
     T *rank;
     T *res;
+    const uint32_t *hub_bits;    // FP32 mode: bit v set when v has an FP64 residual slot
+    const uint32_t *hub_prefix;  // slots before word w of hub_bits
+    double *res_hub;
     float *comp;       // Kahan compensation of rank (FP32 mode only)
     uint32_t *queued;
     uint32_t *q0;
@@ -41,6 +55,73 @@ __device__ __forceinline__ T pr_abs(T x) { return x < T(0) ? -x : x; }
 
 template <class T>
 __device__ __forceinline__ bool pr_finite(T x) { return isfinite(x); }
+
+template <class T>
+__device__ __forceinline__ int32_t hub_slot(const PrArrays<T> &a, uint32_t v) {
+    if (sizeof(T) != 4 || !a.hub_bits) return -1;
+    const uint32_t w = __ldg(a.hub_bits + (v >> 5));
+    const uint32_t b = 1u << (v & 31u);
+    if (!(w & b)) return -1;
+    return static_cast<int32_t>(__ldg(a.hub_prefix + (v >> 5)) + __popc(w & (b - 1u)));
+}
+
+template <class T>
+__device__ __forceinline__ T res_get(const PrArrays<T> &a, uint32_t v) {
+    const int32_t h = hub_slot(a, v);
+    return h >= 0 ? static_cast<T>(__ldcg(a.res_hub + h)) : __ldcg(a.res + v);
+}
+
+template <class T>
+__device__ __forceinline__ void res_set(const PrArrays<T> &a, uint32_t v, double x) {
+    const int32_t h = hub_slot(a, v);
+    if (h >= 0)
+        a.res_hub[h] = x;
+    else
+        a.res[v] = static_cast<T>(x);
+}
+
+// Threshold tests are made in the precision the residual is stored in, so
+// that "crossed epsilon" (queue the vertex) and "above epsilon" (consume it)
+// always agree; a residual left above epsilon but unqueued would never be
+// consumed again.
+
+// Atomic add of c; true when |res| went from <= eps to > eps.
+template <class T>
+__device__ __forceinline__ bool res_add_crossed(const PrArrays<T> &a, uint32_t v, T c, T eps, bool &finite) {
+    const int32_t h = hub_slot(a, v);
+    if (h >= 0) {
+        const double old = atomicAdd(a.res_hub + h, static_cast<double>(c));
+        const double nv = old + static_cast<double>(c);
+        const double e = static_cast<double>(eps);
+        finite = isfinite(nv);
+        return fabs(old) <= e && fabs(nv) > e;
+    }
+    const T old = atomicAdd(a.res + v, c);
+    const T nv = old + c;
+    finite = pr_finite(nv);
+    return pr_abs(old) <= eps && pr_abs(nv) > eps;
+}
+
+// Consume: if |res| > eps, return true with `taken` = the whole residual
+// (FP64 slots keep their full value) and clear it.
+template <class T>
+__device__ __forceinline__ bool res_take(const PrArrays<T> &a, uint32_t v, T eps, double &taken, bool &finite) {
+    const int32_t h = hub_slot(a, v);
+    if (h >= 0) {
+        const double r = __ldcg(a.res_hub + h);
+        finite = isfinite(r);
+        if (!(fabs(r) > static_cast<double>(eps))) return false;
+        taken = r;
+        a.res_hub[h] = 0.0;
+        return true;
+    }
+    const T r = __ldcg(a.res + v);
+    finite = pr_finite(r);
+    if (!(pr_abs(r) > eps)) return false;
+    taken = static_cast<double>(r);
+    a.res[v] = T(0);
+    return true;
+}
 
 template <class T>
 __device__ __forceinline__ T rank_value(const PrArrays<T> &a, uint32_t v) {
@@ -67,7 +148,7 @@ __device__ __forceinline__ void rank_add(const PrArrays<T> &a, uint32_t v, T r) 
 // vertex once when its magnitude crosses epsilon.
 template <class T>
 struct PrPushOp {
-    T *res;
+    PrArrays<T> a;
     uint32_t *queued;
     const T *contrib;
     T eps;
@@ -79,12 +160,10 @@ struct PrPushOp {
     __device__ __forceinline__ bool edge(bool valid, uint32_t, uint32_t item, uint32_t y) const {
         bool want = false;
         if (valid) {
-            const T c = contrib[item];
-            const T old = atomicAdd(res + y, c);
-            const T nv = old + c;
-            if (!pr_finite(nv)) set_error(st, kErrNonFinite, y);
-            if (pr_abs(old) <= eps && pr_abs(nv) > eps && __ldcg(queued + y) == 0u)
+            bool finite = true;
+            if (res_add_crossed(a, y, contrib[item], eps, finite) && __ldcg(queued + y) == 0u)
                 want = atomicCAS(queued + y, 0u, 1u) == 0u;
+            if (!finite) set_error(st, kErrNonFinite, y);
         }
         warp_enqueue(want, y, q_out, q_cnt, cap, st);
         return valid;
@@ -95,7 +174,7 @@ template <class T>
 __global__ void pr_init(PrArrays<T> a, uint32_t n) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
         a.rank[v] = T(0);
-        a.res[v] = T(0.15);
+        res_set(a, v, 0.15);
         if (a.comp) a.comp[v] = 0.f;
         a.queued[v] = 1u;
         a.q0[v] = v;
@@ -113,7 +192,6 @@ __global__ void __launch_bounds__(kTpbPr) pr_converge(AdjView fwd, PrArrays<T> a
                                                       uint32_t *seg_hot, Status *st) {
     __shared__ ExpandSmem<kTpbPr> sm;
     ExpandCounters cnt;
-    const T alpha = sizeof(T) == 4 ? T(kAlphaF) : T(kAlphaD);
     uint32_t r = 0;
     for (;; ++r) {
         const uint32_t n_in = ld_volatile(a.cnt + (r % 3));
@@ -123,19 +201,26 @@ __global__ void __launch_bounds__(kTpbPr) pr_converge(AdjView fwd, PrArrays<T> a
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_in; i += gridDim.x * blockDim.x) {
             const uint32_t v = __ldcg(in + i);
             a.queued[v] = 0u;
-            const T rv = __ldcg(a.res + v);
             T c = T(0);
-            if (!pr_finite(rv)) set_error(st, kErrNonFinite, v);
-            if (pr_abs(rv) > eps) {
-                rank_add(a, v, rv);
-                a.res[v] = T(0);
+            double r64 = 0.0;
+            bool finite = true;
+            if (res_take(a, v, eps, r64, finite)) {
+                // An FP64 residual enters an FP32 rank as two compensated adds
+                // (its float part and the rest), so nothing of it is lost.
+                const T hi = static_cast<T>(r64);
+                rank_add(a, v, hi);
+                if (sizeof(T) == 4) {
+                    const T lo = static_cast<T>(r64 - static_cast<double>(hi));
+                    if (lo != T(0)) rank_add(a, v, lo);
+                }
                 const uint32_t deg = rd_live(fwd.desc[v]);  // out-degree: live entries only
-                if (deg) c = alpha * rv / static_cast<T>(deg);
+                if (deg) c = static_cast<T>(kAlphaD * r64 / static_cast<double>(deg));
             }
+            if (!finite) set_error(st, kErrNonFinite, v);
             a.contrib[i] = c;
         }
         if (!grid_barrier(st)) break;
-        PrPushOp<T> op{a.res, a.queued, a.contrib, eps, (r & 1) ? a.q0 : a.q1, a.cnt + ((r + 1) % 3), a.cap, st};
+        PrPushOp<T> op{a, a.queued, a.contrib, eps, (r & 1) ? a.q0 : a.q1, a.cnt + ((r + 1) % 3), a.cap, st};
         for (uint32_t base = 0; base < n_in; base += gridDim.x * kTpbPr) {
             const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
             bool has = i < n_in;
@@ -147,7 +232,7 @@ __global__ void __launch_bounds__(kTpbPr) pr_converge(AdjView fwd, PrArrays<T> a
                 deg = d.len;
                 off = d.off;
                 has = deg > 0 && __ldcg(a.contrib + i) != T(0);
-                if (has && seg_hot) atomicAdd(seg_hot + (off >> kSegShift), 1u);
+                if (has && seg_hot) atomicAdd(seg_hot + (off >> kSegShift), deg);
             }
             expand_rows<kTpbPr>(fwd, has, v, i, off, deg, op, sm, cnt);
         }
@@ -217,7 +302,7 @@ __global__ void __launch_bounds__(kTpbPr) pr_amend_scatter(AdjView fwd, PrArrays
     __shared__ ExpandSmem<kTpbPr> sm;
     ExpandCounters cnt;
     const uint32_t n = *count;
-    PrPushOp<T> op{a.res, a.queued, contrib, eps, a.q0, a.cnt, a.cap, st};
+    PrPushOp<T> op{a, a.queued, contrib, eps, a.q0, a.cnt, a.cap, st};
     for (uint32_t base = 0; base < n; base += gridDim.x * kTpbPr) {
         const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
         bool has = i < n;
@@ -235,12 +320,101 @@ __global__ void __launch_bounds__(kTpbPr) pr_amend_scatter(AdjView fwd, PrArrays
     flush_counters(st, cnt, kCntPr);
 }
 
+// FP32 mode: a batch's amend (-old contributions over the old rows, +new
+// over the new rows) accumulates per vertex in FP64 and the net change is
+// rounded into the FP32 residual once (pr_amend_fold).  Added straight into
+// FP32 residuals, the two large, mostly cancelling contributions of a hub
+// source leave a rounding residue of ~1e-7 of the contribution behind, which
+// then converges into the ranks as a real error.
+template <class T>
+__global__ void pr_amend_contrib64(const RowDesc *desc, PrArrays<T> a, const uint32_t *list, const uint32_t *count,
+                                   double sign, double *contrib) {
+    const uint32_t n = *count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t s = list[i];
+        const uint32_t deg = rd_live(desc[s]);
+        contrib[i] = deg ? sign * kAlphaD * static_cast<double>(rank_value(a, s)) / static_cast<double>(deg) : 0.0;
+    }
+}
+
+struct PrAmendOp {
+    double *acc;
+    const double *contrib;
+    __device__ __forceinline__ bool edge(bool valid, uint32_t, uint32_t item, uint32_t y) const {
+        if (valid) atomicAdd(acc + y, contrib[item]);
+        return valid;
+    }
+};
+
+template <class T>
+__global__ void __launch_bounds__(kTpbPr) pr_amend_scatter64(AdjView fwd, const uint32_t *list, const uint32_t *count,
+                                                             const double *contrib, double *acc, Status *st) {
+    __shared__ ExpandSmem<kTpbPr> sm;
+    ExpandCounters cnt;
+    const uint32_t n = *count;
+    const PrAmendOp op{acc, contrib};
+    for (uint32_t base = 0; base < n; base += gridDim.x * kTpbPr) {
+        const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
+        bool has = i < n;
+        uint32_t s = 0, deg = 0;
+        uint64_t off = 0;
+        if (has) {
+            s = list[i];
+            const RowDesc d = fwd.desc[s];
+            deg = d.len;
+            off = d.off;
+            has = deg > 0 && contrib[i] != 0.0;
+        }
+        expand_rows<kTpbPr>(fwd, has, s, i, off, deg, op, sm, cnt);
+    }
+    flush_counters(st, cnt, kCntPr);
+}
+
+// Round the accumulated amend into the residuals and queue the vertices
+// whose residual crossed epsilon (Frontier::Add, pr_residual.cuh:16-31).
+template <class T>
+__global__ void pr_amend_fold(PrArrays<T> a, double *acc, uint32_t n, T eps, Status *st) {
+    const uint32_t rounded = (n + 31u) & ~31u;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < rounded; v += gridDim.x * blockDim.x) {
+        bool want = false;
+        if (v < n) {
+            const double d = acc[v];
+            if (d != 0.0) {
+                acc[v] = 0.0;
+                // one thread per vertex: a plain add, crossing tested as in res_add_crossed
+                const int32_t h = hub_slot(a, v);
+                bool crossed, finite;
+                if (h >= 0) {
+                    const double old = a.res_hub[h], nv = old + d, e = static_cast<double>(eps);
+                    a.res_hub[h] = nv;
+                    finite = isfinite(nv);
+                    crossed = fabs(old) <= e && fabs(nv) > e;
+                } else {
+                    const T old = a.res[v];
+                    const T nv = static_cast<T>(static_cast<double>(old) + d);
+                    a.res[v] = nv;
+                    finite = pr_finite(nv);
+                    crossed = pr_abs(old) <= eps && pr_abs(nv) > eps;
+                }
+                if (!finite) set_error(st, kErrNonFinite, v);
+                if (crossed && a.queued[v] == 0u) {
+                    a.queued[v] = 1u;
+                    want = true;
+                }
+            }
+        }
+        warp_enqueue(want, v, a.q0, a.cnt, a.cap, st);
+    }
+}
+
 // FP64 L1 norm of the residual.
 template <class T>
-__global__ void pr_residual_l1(const T *res, uint32_t n, double *out) {
+__global__ void pr_residual_l1(PrArrays<T> a, uint32_t n, double *out) {
     double acc = 0;
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
-        acc += fabs(static_cast<double>(res[v]));
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const int32_t h = hub_slot(a, v);
+        acc += fabs(h >= 0 ? a.res_hub[h] : static_cast<double>(a.res[v]));
+    }
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
     if (lane_id() == 0 && acc != 0.0) atomicAdd(out, acc);
 }
@@ -250,9 +424,9 @@ __global__ void pr_export(PrArrays<T> a, uint32_t n, float *rank, float *res, do
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
         const T x = rank_value(a, v);
         if (rank) rank[v] = static_cast<float>(x);
-        if (res) res[v] = static_cast<float>(__ldcg(a.res + v));
+        if (res) res[v] = static_cast<float>(res_get(a, v));
         if (rank64) rank64[v] = static_cast<double>(x);
-        if (res64) res64[v] = static_cast<double>(__ldcg(a.res + v));
+        if (res64) res64[v] = static_cast<double>(res_get(a, v));
     }
 }
 

@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(kTpbMs) ms_closure(AdjView fwd, uint32_t *dist
         uint32_t *out = (r & 1) ? fr.q0 : fr.q1;
         unsigned long long *m_in = (r & 1) ? fr.mask1 : fr.mask0;
         unsigned long long *m_out = (r & 1) ? fr.mask0 : fr.mask1;
-        const Defer df{big.rows, big.cnt + (r % 3), big.cap};
+        const Defer df{big.rows, big.cnt + (r % 3), big.cap, big.split};
         for (uint32_t base = 0; base < n_in; base += gridDim.x * kTpbMs) {
             const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
             bool has = i < n_in;
@@ -206,6 +206,20 @@ __global__ void ms_transpose(const uint32_t *dist, uint32_t n, uint32_t width, u
         const uint32_t j = e / kMsTile, vv = e % kMsTile;
         if (vv < rows) out[static_cast<uint64_t>(j) * n + v0 + vv] = tile[vv][j];
     }
+}
+
+// Digest of every row of a k x n result (the function of value_digest, so a
+// query row and a maintained state with the same values agree).
+__global__ void ms_row_digest(const uint32_t *rows, uint32_t n, unsigned long long *out) {
+    const uint32_t j = blockIdx.y;
+    const uint32_t *row = rows + static_cast<uint64_t>(j) * n;
+    unsigned long long acc = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const uint32_t d = row[v];
+        if (d != kInf) acc += digest_mix((static_cast<unsigned long long>(v) << 32) | d);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
+    if (lane_id() == 0 && acc) atomicAdd(out + j, acc);
 }
 
 }  // namespace cig

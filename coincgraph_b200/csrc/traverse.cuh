@@ -139,6 +139,7 @@ struct BigList {
     BigRow *rows;
     uint32_t *cnt;  // 3 counters
     uint32_t cap;
+    uint32_t split;  // deferral threshold (row entries), tuned per handle
 };
 
 template <int A>
@@ -163,7 +164,7 @@ __global__ void __launch_bounds__(kTpb) push_closure(AdjView fwd, unsigned long 
         }
         const uint32_t *in = (r & 1) ? fr.q1 : fr.q0;
         PushOp<A> op{state, qstamp, tag0 + r, (r & 1) ? fr.q0 : fr.q1, fr.cnt + ((r + 1) % 3), fr.cap, st};
-        const Defer df{big.rows, big.cnt + (r % 3), big.cap};
+        const Defer df{big.rows, big.cnt + (r % 3), big.cap, big.split};
         // Item i goes to block i mod gridDim.x, so small frontiers still
         // spread over the whole grid.
         for (uint32_t base = 0; base < n_in; base += gridDim.x * kTpb) {
@@ -178,7 +179,7 @@ __global__ void __launch_bounds__(kTpb) push_closure(AdjView fwd, unsigned long 
                 deg = d.len;
                 off = d.off;
                 has = dx != kInf && deg > 0;
-                if (has && seg_hot) atomicAdd(seg_hot + (off >> kSegShift), 1u);
+                if (has && seg_hot) atomicAdd(seg_hot + (off >> kSegShift), deg);
             }
             expand_rows<kTpb>(fwd, has, x, dx, off, deg, op, sm, cnt, df);
         }
@@ -203,7 +204,7 @@ template <int A>
 __global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long long *state, uint32_t *aff_stamp,
                                                       uint32_t epoch, uint32_t *list, uint32_t *cnt3,
                                                       uint32_t cap, BigList big, uint32_t max_rounds,
-                                                      uint32_t *aff_total, Status *st) {
+                                                      uint32_t *aff_total, uint32_t *seg_hot, Status *st) {
     __shared__ ExpandSmem<kTpb> sm;
     ExpandCounters c;
     uint32_t lo = 0, hi = ld_volatile(cnt3 + 0);
@@ -219,7 +220,7 @@ __global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long
             big.cnt[(r + 2) % 3] = 0;
         }
         InvalOp<A> op{state, aff_stamp, epoch, list + hi, cnt3 + ((r + 1) % 3), cap > hi ? cap - hi : 0u, st};
-        const Defer df{big.rows, big.cnt + (r % 3), big.cap};
+        const Defer df{big.rows, big.cnt + (r % 3), big.cap, big.split};
         const uint32_t n_in = hi - lo;
         for (uint32_t base = 0; base < n_in; base += gridDim.x * kTpb) {
             const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
@@ -233,6 +234,7 @@ __global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long
                 deg = d.len;
                 off = d.off;
                 has = deg > 0;
+                if (has && seg_hot) atomicAdd(seg_hot + (off >> kSegShift), deg);
             }
             expand_rows<kTpb>(fwd, has, x, px, off, deg, op, sm, c, df);
         }
@@ -299,7 +301,7 @@ __global__ void __launch_bounds__(kTpb) pull_repair(AdjView rev, unsigned long l
     ExpandCounters c;
     const uint32_t n = *total;
     PullOp<A> op{state, aff_stamp, epoch};
-    const Defer df{big.rows, big.cnt, big.cap};
+    const Defer df{big.rows, big.cnt, big.cap, big.split};
     for (uint32_t base = 0; base < n; base += gridDim.x * kTpb) {
         const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
         bool has = i < n;

@@ -19,6 +19,7 @@ BFS, SSSP, CC, PR = 0, 1, 2, 3
 ALGOS = {"bfs": BFS, "sssp": SSSP, "cc": CC, "pr": PR}
 FLAG_NO_CACHE_REFRESH = 0x1
 FLAG_PR_FP64 = 0x2
+FLAG_WEIGHT_U255 = 0x4
 INF = 0xFFFFFFFF
 
 STATUS = {
@@ -88,6 +89,69 @@ class GraphInfo(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class UpdateBatch(ctypes.Structure):
+    _fields_ = [
+        ("del_u", ctypes.c_void_p),
+        ("del_v", ctypes.c_void_p),
+        ("nd", ctypes.c_uint64),
+        ("add_u", ctypes.c_void_p),
+        ("add_v", ctypes.c_void_p),
+        ("na", ctypes.c_uint64),
+    ]
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [
+        ("blocks_per_sm", ctypes.c_uint32),
+        ("split_degree", ctypes.c_uint32),
+        ("best_ms", ctypes.c_double),
+        ("candidates", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "pad"}
+
+
+REQ_UPDATE, REQ_BFS, REQ_SSSP = 0, 1, 2
+
+
+class Request(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int32),
+        ("source", ctypes.c_uint32),
+        ("del_u", ctypes.c_void_p),
+        ("del_v", ctypes.c_void_p),
+        ("nd", ctypes.c_uint64),
+        ("add_u", ctypes.c_void_p),
+        ("add_v", ctypes.c_void_p),
+        ("na", ctypes.c_uint64),
+        ("out", ctypes.c_void_p),
+    ]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int32),
+        ("wave", ctypes.c_uint32),
+        ("digest", ctypes.c_uint64),
+        ("submit_ms", ctypes.c_double),
+        ("start_ms", ctypes.c_double),
+        ("done_ms", ctypes.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class ServeOptions(ctypes.Structure):
+    _fields_ = [
+        ("budget_bytes", ctypes.c_uint64),
+        ("max_wave", ctypes.c_uint32),
+        ("max_pending", ctypes.c_uint32),
+    ]
+
+
 class QueryStats(ctypes.Structure):
     _fields_ = [
         ("ms", ctypes.c_double),
@@ -104,7 +168,8 @@ class QueryStats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
-STAGES = ["group", "mutate", "seed", "inval", "pull", "push", "pr", "cache", "mutate_rev", "add", "add_rev"]
+STAGES = ["group", "mutate", "seed", "inval", "pull", "push", "pr", "cache", "mutate_rev", "add", "add_rev",
+          "del_scan"]
 
 
 class StageProfile(ctypes.Structure):
@@ -149,6 +214,13 @@ SIGNATURES = [
     ("cig_profile_enable", _i32, [_vp, _i32]),
     ("cig_profile_read", _i32, [_vp, ctypes.POINTER(StageProfile), _u32]),
     ("cig_bfs_csr_noalloc", _i32, [_vp, _vp, _u32, _u32, _vp, _vp]),
+    ("cig_apply_batches_device", _i32, [_vp, ctypes.POINTER(UpdateBatch), _u32, ctypes.POINTER(BatchStats), _vp]),
+    ("cig_autotune", _i32, [_vp, ctypes.POINTER(TuneResult)]),
+    ("cig_serve_start", _i32, [_vp, ctypes.POINTER(ServeOptions)]),
+    ("cig_serve_submit", _i32, [_vp, ctypes.POINTER(Request), ctypes.POINTER(_u64)]),
+    ("cig_serve_wait", _i32, [_vp, _u64, ctypes.POINTER(Result)]),
+    ("cig_serve_poll", _i32, [_vp, _u64, ctypes.POINTER(Result), ctypes.POINTER(ctypes.c_int)]),
+    ("cig_serve_stop", _i32, [_vp]),
     ("cig_query_bfs_multi", _i32, [_vp, _vp, _u32, _vp]),
     ("cig_query_sssp_multi", _i32, [_vp, _vp, _u32, _vp]),
     ("cig_query_multi_device", _i32, [_vp, _i32, _vp, _u32, _u32, _vp, ctypes.POINTER(QueryStats)]),
@@ -292,6 +364,20 @@ class Engine:
                                                     ctypes.byref(s)))
         return s
 
+    def apply_batches_device(self, batches, digests: bool = True):
+        """The batched form: a list of (du, dv, au, av) device arrays applied
+        with one synchronisation; returns per-batch stats and digests."""
+        arr = (UpdateBatch * max(len(batches), 1))()
+        for i, (du, dv, au, av) in enumerate(batches):
+            nd = int(du.numel()) if hasattr(du, "numel") else len(du)
+            na = int(au.numel()) if hasattr(au, "numel") else len(au)
+            arr[i] = UpdateBatch(_ptr(du), _ptr(dv), nd, _ptr(au), _ptr(av), na)
+        st = (BatchStats * max(len(batches), 1))()
+        dg = np.zeros(max(len(batches), 1), dtype=np.uint64)
+        self._check(self.lib.cig_apply_batches_device(self.h, arr, len(batches), st,
+                                                      _ptr(dg) if digests else None))
+        return [st[i] for i in range(len(batches))], [int(x) for x in dg[: len(batches)]]
+
     # -- results
     def values(self) -> np.ndarray:
         out = np.empty(self.n, dtype=np.uint32)
@@ -313,6 +399,55 @@ class Engine:
             s = np.empty(self.n, dtype=np.float32)
             self._check(self.lib.cig_get_pr(self.h, _ptr(r), _ptr(s)))
         return r, s
+
+    def autotune(self) -> dict:
+        r = TuneResult()
+        self._check(self.lib.cig_autotune(self.h, ctypes.byref(r)))
+        return r.as_dict()
+
+    # -- serving
+    def serve_start(self, budget_bytes: int = 0, max_wave: int = 0, max_pending: int = 0):
+        o = ServeOptions(budget_bytes, max_wave, max_pending)
+        self._check(self.lib.cig_serve_start(self.h, ctypes.byref(o)))
+        self._keep = {}
+
+    def _serve_check(self, rc: int):
+        if rc != 0:
+            raise CigError(rc, self.lib.cig_last_error(None).decode(errors="replace"))
+
+    def submit_update(self, du, dv, au, av) -> int:
+        du, dv, au, av = _u32arr(du), _u32arr(dv), _u32arr(au), _u32arr(av)
+        r = Request(REQ_UPDATE, 0, _ptr(du), _ptr(dv), len(du), _ptr(au), _ptr(av), len(au), None)
+        t = ctypes.c_uint64()
+        self._serve_check(self.lib.cig_serve_submit(self.h, ctypes.byref(r), ctypes.byref(t)))
+        return t.value
+
+    def submit_query(self, algo: str, source: int, out: np.ndarray | None = None) -> int:
+        kind = REQ_BFS if algo == "bfs" else REQ_SSSP
+        r = Request(kind, int(source), None, None, 0, None, None, 0, _ptr(out) if out is not None else None)
+        t = ctypes.c_uint64()
+        self._serve_check(self.lib.cig_serve_submit(self.h, ctypes.byref(r), ctypes.byref(t)))
+        if out is not None:
+            self._keep[t.value] = out  # the library writes into it when the wave ends
+        return t.value
+
+    def wait(self, ticket: int) -> dict:
+        res = Result()
+        self._serve_check(self.lib.cig_serve_wait(self.h, ticket, ctypes.byref(res)))
+        self._keep.pop(ticket, None)
+        return res.as_dict()
+
+    def poll(self, ticket: int):
+        res = Result()
+        done = ctypes.c_int()
+        self._serve_check(self.lib.cig_serve_poll(self.h, ticket, ctypes.byref(res), ctypes.byref(done)))
+        if done.value:
+            self._keep.pop(ticket, None)
+            return res.as_dict()
+        return None
+
+    def serve_stop(self):
+        self._check(self.lib.cig_serve_stop(self.h))
 
     # -- multi-source queries on the current graph
     def query_bfs(self, sources) -> np.ndarray:

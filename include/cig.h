@@ -60,6 +60,9 @@ typedef struct {
 
 #define CIG_FLAG_NO_CACHE_REFRESH 0x1u /* keep the segment residency chosen at load */
 #define CIG_FLAG_PR_FP64 0x2u          /* PR ranks/residuals in FP64 (default: FP32 + Kahan) */
+#define CIG_FLAG_WEIGHT_U255 0x4u      /* SSSP weights uniform in [1, 255]: 1 + lowbias32(u*0x9E3779B1 +
+                                          v*0x85EBCA77) mod 255 (an extension; the reference's SSSP
+                                          weight is (u+v)%128+1 whatever the file holds) */
 
 typedef struct {
     uint64_t requested_deletes;
@@ -139,6 +142,98 @@ int cig_apply_batch_device(cig_handle *h, const uint32_t *del_u, const uint32_t 
                            const uint32_t *add_u, const uint32_t *add_v, uint64_t na,
                            cig_batch_stats *stats);
 
+/* One update batch of device-resident arrays (for cig_apply_batches_device). */
+typedef struct {
+    const uint32_t *del_u;
+    const uint32_t *del_v;
+    uint64_t nd;
+    const uint32_t *add_u;
+    const uint32_t *add_v;
+    uint64_t na;
+} cig_update_batch;
+
+/* The batched form of cig_apply_batch_device: `count` batches of any sizes
+ * queued back to back with one host synchronisation at the end, so the
+ * launches of batch i+1 overlap the execution of batch i.  Each batch is
+ * applied completely (deletion phase, insertion phase, repair, cache
+ * service) before the next, exactly as by `count` single calls.  stats[i]
+ * (optional) gets batch i's counters and stage times; digests[i] (optional,
+ * not for PR) the cig_value_digest of the values after batch i.  No
+ * reference counterpart (the reference synchronises with the host every
+ * round of every batch). */
+int cig_apply_batches_device(cig_handle *h, const cig_update_batch *batches, uint32_t count,
+                             cig_batch_stats *stats, uint64_t *digests);
+
+/* Launch-shape autotuner: times the static solve on the loaded graph for
+ * cooperative blocks per SM in {2, 4, 8} (the frontier tile of the persistent
+ * closures) x hub-row split degree in {1024, 4096, 16384} (rows at least that
+ * long are expanded by the whole grid in 1024-entry chunks) and keeps the
+ * fastest for the handle.  Values are unchanged (the solve's values are
+ * unique).  BFS/SSSP/CC.  No reference counterpart (the reference's
+ * --lb_push/--lb_pull/--block_size hints have no effect). */
+typedef struct {
+    uint32_t blocks_per_sm;
+    uint32_t split_degree;
+    double best_ms;
+    uint32_t candidates;
+    uint32_t pad;
+} cig_tune_result;
+
+int cig_autotune(cig_handle *h, cig_tune_result *res);
+
+/* ---------------------------------------------------------------- serving
+ * A request loop on one handle: update batches and BFS/SSSP queries are
+ * submitted from any host thread and served in submission order (a query
+ * sees every update submitted before it and none after).  Consecutive
+ * queries of one kind are answered together as one bitmask wave (up to
+ * max_wave sources: continuous batching), a wave overlaps the copy and key
+ * sort of the update that follows it, and requests are admitted by their
+ * device-memory footprint: an update larger than the budget allows is
+ * applied as consecutive deletion chunks then insertion chunks (the same
+ * rows and values as one batch).  While serving, the handle's other calls
+ * return CIG_ERR_STATE; the serve calls may come from any threads and report
+ * their errors through cig_last_error(NULL) of the calling thread.  Every
+ * ticket's result is taken once (wait or poll) before cig_serve_stop.  No
+ * reference counterpart (the reference samples replay a file of batches). */
+typedef enum { CIG_REQ_UPDATE = 0, CIG_REQ_BFS = 1, CIG_REQ_SSSP = 2 } cig_request_kind;
+
+typedef struct {
+    int32_t kind;             /* cig_request_kind */
+    uint32_t source;          /* queries: source vertex */
+    const uint32_t *del_u;    /* updates: host arrays, copied by cig_serve_submit */
+    const uint32_t *del_v;
+    uint64_t nd;
+    const uint32_t *add_u;
+    const uint32_t *add_v;
+    uint64_t na;
+    uint32_t *out;            /* queries: n words of host memory for the depths/distances, or NULL */
+} cig_request;
+
+typedef struct {
+    int32_t status;           /* CIG_OK or the request's error */
+    uint32_t wave;            /* queries: sources answered in the same wave */
+    uint64_t digest;          /* updates: cig_value_digest after the batch (not PR);
+                                 queries: order-independent digest of the result row */
+    double submit_ms;         /* times since cig_serve_start */
+    double start_ms;
+    double done_ms;
+} cig_result;
+
+typedef struct {
+    uint64_t budget_bytes;    /* device bytes for per-request buffers (0: half of the free memory) */
+    uint32_t max_wave;        /* sources per query wave, 1..64 (0: 64) */
+    uint32_t max_pending;     /* submitted, unfinished requests before submit blocks (0: 4096) */
+} cig_serve_options;
+
+int cig_serve_start(cig_handle *h, const cig_serve_options *o);
+int cig_serve_submit(cig_handle *h, const cig_request *r, uint64_t *ticket);
+/* Block until request `ticket` is done and return its result (once). */
+int cig_serve_wait(cig_handle *h, uint64_t ticket, cig_result *res);
+/* Non-blocking: *done = 1 and the result when finished, else *done = 0. */
+int cig_serve_poll(cig_handle *h, uint64_t ticket, cig_result *res, int *done);
+/* Serve what is pending, then stop the loop; the handle is usable again. */
+int cig_serve_stop(cig_handle *h);
+
 /* Replaces GatherValue / GatherParent (framework.cuh:2896-2916): BFS depth,
  * SSSP distance or CC label; parents (0xFFFFFFFF for none). */
 int cig_get_values(cig_handle *h, uint32_t *out);
@@ -207,7 +302,10 @@ enum {
     CIG_STAGE_MUTATE_REV = 8, /* reverse (in-edge) rows */
     CIG_STAGE_ADD = 9,        /* forward rows, addition phase (MUTATE is then the deletion phase) */
     CIG_STAGE_ADD_REV = 10,   /* reverse rows, addition phase */
-    CIG_STAGE_COUNT = 11
+    CIG_STAGE_DEL_SCAN = 11,  /* the flat deletion scan kernel alone (inside MUTATE and MUTATE_REV):
+                                 edges = row entries read, edges_cached = of which from HBM,
+                                 hits = deletion keys of the scanned rows */
+    CIG_STAGE_COUNT = 12
 };
 
 typedef struct {

@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libcigref.so")
 
-BFS, SSSP, CC = 0, 1, 2
+BFS, SSSP, CC, SSSP_U255 = 0, 1, 2, 3
 INF = 0xFFFFFFFF
 
 _vp, _u32, _u64, _i32, _dbl = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int, ctypes.c_double

@@ -145,6 +145,17 @@ uint64_t og_add(og_graph *g, const uint32_t *u, const uint32_t *v, uint64_t m) {
 uint32_t og_weight(int mode, uint32_t u, uint32_t v) {
     if (mode == OG_BFS) return 1;
     if (mode == OG_CC) return 0;
+    if (mode == OG_SSSP_U255) {
+        /* the extension's weights in [1, 255]: lowbias32 (C. Wellons) of a
+         * linear mix of the ids, as the engine's weight_u255 */
+        uint32_t x = u * 0x9E3779B1u + v * 0x85EBCA77u;
+        x ^= x >> 16;
+        x *= 0x7FEB352Du;
+        x ^= x >> 15;
+        x *= 0x846CA68Bu;
+        x ^= x >> 16;
+        return 1u + x % 255u;
+    }
     return (uint32_t)(((uint64_t)u + v) % 128 + 1);
 }
 
@@ -203,7 +214,7 @@ void og_sssp_fifo(const og_graph *g, uint32_t src, int mode, uint32_t *dist, uin
 
 /*
  * Independent cross-check: Dial's bucket-queue Dijkstra (weights are at most
- * 128), so that two unrelated algorithms agree on every distance.
+ * 255 < NB buckets), so that two unrelated algorithms agree on every distance.
  */
 void og_sssp_dial(const og_graph *g, uint32_t src, int mode, uint32_t *dist) {
     const uint32_t n = g->n;

@@ -31,7 +31,7 @@ extern "C" {
 
 #define OG_INF 0xFFFFFFFFu
 
-enum { OG_BFS = 0, OG_SSSP = 1, OG_CC = 2 };
+enum { OG_BFS = 0, OG_SSSP = 1, OG_CC = 2, OG_SSSP_U255 = 3 };
 
 typedef struct og_graph og_graph;
 

@@ -137,7 +137,18 @@ def heavy_delete_case() -> Case:
     return Case("heavydelete", n, xadj, adj, batches, source=0)
 
 
-ORACLE_MODE = {"bfs": 0, "sssp": 1, "cc": 2}
+ORACLE_MODE = {"bfs": 0, "sssp": 1, "cc": 2, "sssp_u255": 3}
+
+
+def make_engine(algo: str, **kw):
+    """Engine for a test algorithm name; "sssp_u255" is SSSP with the
+    uniform [1, 255] edge weights (CIG_FLAG_WEIGHT_U255)."""
+    from coincgraph_b200 import Engine
+    from coincgraph_b200.engine import FLAG_WEIGHT_U255
+
+    if algo == "sssp_u255":
+        return Engine("sssp", flags=kw.pop("flags", 0) | FLAG_WEIGHT_U255, **kw)
+    return Engine(algo, **kw)
 
 
 def oracle_trace(case: Case, algo: str):

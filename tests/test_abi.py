@@ -59,3 +59,8 @@ def test_struct_layouts(built):
     assert ctypes.sizeof(engine.BatchStats) == 20 * 8
     assert ctypes.sizeof(engine.StageProfile) == 6 * 8
     assert ctypes.sizeof(engine.QueryStats) == 8 * 8
+    assert ctypes.sizeof(engine.UpdateBatch) == 6 * 8
+    assert ctypes.sizeof(engine.Request) == 8 * 8
+    assert ctypes.sizeof(engine.Result) == 5 * 8
+    assert ctypes.sizeof(engine.ServeOptions) == 16
+    assert ctypes.sizeof(engine.TuneResult) == 24

@@ -115,6 +115,24 @@ def test_traversal_tool_end_to_end(dataset, name, mode):
 
 
 @pytest.mark.gpu
+def test_sssp_tool_extensions(dataset):
+    """--weight_u255 (weights in [1, 255]), --write_cigb then a run from the
+    binary sidecar, and --autotune: checks pass and distances match the
+    oracle with the same weights."""
+    g, ups, graph, upd, sizes, tmp = dataset
+    out = tmp / "out_u255.txt"
+    common = [f"--updatefile={upd}", f"--update_size={sizes}", "--cache=2", "--check=true", "--weight_u255=true"]
+    r = run("sssp", f"--graphfile={graph}", "--write_cigb=true", "--autotune=true", *common)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr
+    assert os.path.exists(graph + ".cigb") and "[AUTOTUNE] blocks_per_sm=" in r.stdout
+    r = run("sssp", f"--graphfile={graph}", f"--output={out}", *common)
+    assert r.returncode == 0 and "Overall: Test passed" in r.stdout, r.stdout[-2000:] + r.stderr
+    cols = np.loadtxt(out, dtype=np.uint64)
+    og = _oracle_final(g, ups, oracle.SSSP_U255)
+    assert np.array_equal(cols[:, 1].astype(np.uint32), og.sssp(0, oracle.SSSP_U255))
+
+
+@pytest.mark.gpu
 def test_cc_tool_end_to_end(dataset):
     g, ups, graph, upd, sizes, tmp = dataset
     out = tmp / "labels.txt"

@@ -13,7 +13,8 @@ import pytest
 
 import oracle
 from coincgraph_b200 import Engine
-from helpers import ORACLE_MODE, adversarial_case, big_row_case, heavy_delete_case, oracle_trace, rmat_case
+from helpers import (ORACLE_MODE, adversarial_case, big_row_case, heavy_delete_case, make_engine, oracle_trace,
+                     rmat_case)
 
 pytestmark = pytest.mark.gpu
 
@@ -34,7 +35,7 @@ def _check_values(eng, g, case, algo, expect, where):
 def run_case(case, algo, cache_gib):
     trace, _ = oracle_trace(case, algo)
     g = oracle.Graph(case.n, case.xadj, case.adj)
-    with Engine(algo, source=case.source, cache_gib=cache_gib) as eng:
+    with make_engine(algo, source=case.source, cache_gib=cache_gib) as eng:
         eng.load_csr(case.n, case.xadj, case.adj)
         eng.init()
         _check_values(eng, g, case, algo, trace["init"], "after init")
@@ -115,6 +116,89 @@ def test_whole_batch_equals_phases(algo):
             assert a.digest() == b.digest()
 
 
+def run_case_whole_batches(case, algo, cache_gib):
+    """Batches through cig_apply_batch (one key sort for the whole batch and
+    the per-batch segment-table service); values and rows after every batch."""
+    trace, _ = oracle_trace(case, algo)
+    g = oracle.Graph(case.n, case.xadj, case.adj)
+    stats = []
+    with make_engine(algo, source=case.source, cache_gib=cache_gib) as eng:
+        eng.load_csr(case.n, case.xadj, case.adj)
+        eng.init()
+        for i, (du, dv, au, av) in enumerate(case.batches):
+            missing = g.delete(du, dv)
+            invalid = g.add(au, av)
+            s = eng.apply_batch(du, dv, au, av)
+            assert s["missing_deletes"] == missing and s["invalid_additions"] == invalid
+            stats.append(s)
+            _check_values(eng, g, case, algo, trace["batch"][i], f"after batch {i}")
+            xadj, adj = eng.export_csr()
+            assert np.array_equal(xadj, trace["rows"][i][0]) and np.array_equal(adj, trace["rows"][i][1])
+    return stats
+
+
+@pytest.mark.parametrize("algo", ["bfs", "sssp", "cc"])
+@pytest.mark.parametrize("cache", list(CACHES))
+def test_rmat_stream_whole_batches(algo, cache):
+    run_case_whole_batches(rmat_case(11, 4, 300, 300, seed_offset=14), algo, CACHES[cache])
+
+
+@pytest.mark.parametrize("cache", ["resident", "mixed"])
+def test_uniform_255_weights(cache):
+    """The [1, 255] weight extension against the oracle's same weights."""
+    run_case(rmat_case(11, 3, 300, 300, seed_offset=16), "sssp_u255", CACHES[cache])
+    run_case_whole_batches(heavy_delete_case(), "sssp_u255", CACHES[cache])
+
+
+@pytest.mark.parametrize("algo", ["sssp", "cc"])
+def test_adversarial_and_big_rows_whole_batches(algo):
+    run_case_whole_batches(adversarial_case(), algo, CACHES["mixed"])
+    run_case_whole_batches(big_row_case(), algo, CACHES["mixed"])
+
+
+@pytest.mark.parametrize("algo", ["bfs", "sssp"])
+def test_segment_table_churn(algo, monkeypatch):
+    """Every segment counts as cold and every touched host segment as hot, so
+    each batch evicts (writing dirty segments back) and admits segments; the
+    results and rows must not change."""
+    monkeypatch.setenv("CIG_CACHE_ADMIT_SCORE", "1")
+    monkeypatch.setenv("CIG_CACHE_COLD_SCORE", str(1 << 30))
+    stats = run_case_whole_batches(rmat_case(14, 6, 2000, 2000, seed_offset=15), algo, 8 * ONE_SEGMENT_GIB)
+    assert sum(s["cache_segments_evicted"] for s in stats) > 0
+    assert sum(s["cache_segments_loaded"] for s in stats) > 0
+
+
+@pytest.mark.parametrize("algo", ["bfs", "sssp", "cc"])
+def test_batched_form_equals_single_batches(algo):
+    """cig_apply_batches_device (uneven batch sizes, one synchronisation)
+    leaves every batch's values (digest per batch) and the final rows and
+    values equal to one cig_apply_batch call per batch."""
+    import torch
+
+    from coincgraph_b200 import gen
+
+    g, h = gen.rmat(12, keep_handle=True)
+    sizes = [7, 900, 60, 0, 2500, 1]
+    ups = gen.updates(h, sizes, sizes[::-1], seed=gen.UPDATE_SEED_BASE + 140)
+    batches = [ups.batch(i) for i in range(len(sizes))]
+    with Engine(algo, cache_gib=2 * ONE_SEGMENT_GIB) as a, Engine(algo, cache_gib=2 * ONE_SEGMENT_GIB) as b:
+        for e in (a, b):
+            e.load_csr(g.n, g.xadj, g.adj)
+            e.init()
+        expect = []
+        for du, dv, au, av in batches:
+            a.apply_batch(du, dv, au, av)
+            expect.append(a.digest())
+        dev = [[torch.from_numpy(x.astype(np.int32)).cuda() for x in bt] for bt in batches]
+        stats, digests = b.apply_batches_device(dev)
+        assert digests == expect
+        assert [s.requested_deletes for s in stats] == sizes
+        assert np.array_equal(a.values(), b.values())
+        xa, aa = a.export_csr()
+        xb, ab = b.export_csr()
+        assert np.array_equal(xa, xb) and np.array_equal(aa, ab)
+
+
 def test_device_inputs_match_host_inputs():
     import torch
 
@@ -170,3 +254,20 @@ def test_arena_exhaustion_is_an_error_not_a_fault():
                 av = rng.integers(0, n, 5000).astype(np.uint32)
                 eng.apply_batch([], [], au, av)
         assert err.value.code == -4
+
+
+def test_autotune_keeps_values_and_parity():
+    """cig_autotune re-runs the static solve under each launch shape; the
+    values stay the same and later batches still match the oracle."""
+    case = rmat_case(12, 3, 500, 500, seed_offset=17)
+    trace, _ = oracle_trace(case, "sssp")
+    with Engine("sssp", cache_gib=4.0) as eng:
+        eng.load_csr(case.n, case.xadj, case.adj)
+        eng.init()
+        before = eng.values()
+        r = eng.autotune()
+        assert r["candidates"] == 9 and r["blocks_per_sm"] in (2, 4, 8) and r["split_degree"] in (1024, 4096, 16384)
+        assert np.array_equal(eng.values(), before)
+        for i, b in enumerate(case.batches):
+            eng.apply_batch(*b)
+            assert np.array_equal(eng.values(), trace["batch"][i])

@@ -11,7 +11,7 @@ import pytest
 import oracle
 from coincgraph_b200 import Engine
 from coincgraph_b200.engine import FLAG_PR_FP64
-from helpers import adversarial_case, rmat_case
+from helpers import adversarial_case, big_row_case, rmat_case
 
 pytestmark = pytest.mark.gpu
 
@@ -21,7 +21,8 @@ def max_rel(x, ref):
 
 
 @pytest.mark.parametrize("fp64,eps,tol", [(False, 1e-9, 1e-5), (True, 1e-13, 1e-9)])
-@pytest.mark.parametrize("make", [lambda: rmat_case(10, 4, 200, 200, seed_offset=20), adversarial_case])
+@pytest.mark.parametrize("make", [lambda: rmat_case(10, 4, 200, 200, seed_offset=20), adversarial_case,
+                                  big_row_case])
 def test_pr_stream(make, fp64, eps, tol):
     case = make()
     g = oracle.Graph(case.n, case.xadj, case.adj)

@@ -86,6 +86,21 @@ def test_query_hub_rows_and_width_forms(built):
         np.testing.assert_array_equal(outs[64][j], og.sssp(int(s), oracle.SSSP))
 
 
+def test_query_sssp_uniform_255_weights(built):
+    from coincgraph_b200.engine import FLAG_WEIGHT_U255
+
+    g = gen.rmat(11)
+    src = _sources(g, 20)
+    og = oracle.Graph(g.n, g.xadj, g.adj)
+    with Engine("sssp", cache_gib=1.0, flags=FLAG_WEIGHT_U255) as eng:
+        eng.load_csr(g.n, g.xadj, g.adj)
+        eng.init()
+        got = eng.query_sssp(src)
+        np.testing.assert_array_equal(eng.values(), og.sssp(0, oracle.SSSP_U255))
+    for j, s in enumerate(src):
+        np.testing.assert_array_equal(got[j], og.sssp(int(s), oracle.SSSP_U255))
+
+
 def test_query_rejects_bad_arguments(built):
     from coincgraph_b200 import CigError
 

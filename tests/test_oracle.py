@@ -103,7 +103,7 @@ def test_pagerank_passes_reference_checker(built):
     assert g.pr_check(bad, residual, 1e-6)["ok"] == 0.0
 
 
-@pytest.mark.parametrize("mode", [oracle.BFS, oracle.SSSP])
+@pytest.mark.parametrize("mode", [oracle.BFS, oracle.SSSP, oracle.SSSP_U255])
 def test_two_sssp_oracles_agree(built, mode):
     case = rmat_case(11, 2, 200, 200, seed_offset=6)
     g = oracle.Graph(case.n, case.xadj, case.adj)
@@ -153,3 +153,16 @@ def test_checksum_restates_reference_formula(built):
         h ^= (v + 0x9E3779B97F4A7C15 + (d << 6) + (d >> 2)) & mask
         h = (h * 1099511628211) & mask
     assert oracle.checksum(vals) == h
+
+
+def test_uniform_255_weights_cover_the_range(built):
+    """The extension's weight function spans [1, 255] about evenly."""
+    import ctypes
+
+    lib = oracle.lib()
+    lib.og_weight.restype = ctypes.c_uint32
+    lib.og_weight.argtypes = [ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32]
+    w = np.array([lib.og_weight(oracle.SSSP_U255, u, v) for u in range(60) for v in range(60)])
+    assert w.min() == 1 and w.max() == 255
+    counts = np.bincount(w, minlength=256)[1:]
+    assert counts.min() > 0 and counts.max() < 4 * counts.mean()
