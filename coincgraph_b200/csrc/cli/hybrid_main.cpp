@@ -711,8 +711,8 @@ static bool run() {
     if (B("autotune")) {
         cig_tune_result tr;
         ck(cig_autotune(g_h, &tr), "cig_autotune");
-        LOG("[AUTOTUNE] blocks_per_sm=%u split_degree=%u solve_ms=%.3f candidates=%u\n", tr.blocks_per_sm,
-            tr.split_degree, tr.best_ms, tr.candidates);
+        LOG("[AUTOTUNE] blocks_per_sm=%u split_degree=%u pull_divisor=%u solve_ms=%.3f candidates=%u\n",
+            tr.blocks_per_sm, tr.split_degree, tr.pull_divisor, tr.best_ms, tr.candidates);
     }
 #endif
     bool success = true;

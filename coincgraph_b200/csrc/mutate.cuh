@@ -602,15 +602,14 @@ __global__ void del_classify(const RowDesc *desc, const unsigned long long *keys
 // Each chunk records the first live match of every key (atomicMin).
 //
 // Membership test per row entry, by the row's number of requests: up to
-// kDelLaneKeys, compare against the keys held in lanes (about 9 instructions
-// per request per 4 entries); up to kDelCmpKeys, a 64-bit filter in a
-// register (6-bit hash) and a linear check of the keys in shared memory on a
-// filter hit; beyond, a per-warp bit filter in shared memory (32 bits per
-// request rounded up to a power of two, 1024..16384 bits) and a binary search
-// on a hit.  Filters are built once per group, so most entries are rejected
-// by one test and only filter hits pay the exact search.
-constexpr uint32_t kDelLaneKeys = 2;  // up to this many requests: compare against lane registers
-constexpr uint32_t kDelCmpKeys = 8;   // up to this many: 64-bit register filter, else the shared-memory filter
+// kDelCmpKeys, compare against the keys held in lanes (about 9 instructions
+// per request per 4 entries, no divergence); beyond, a per-warp bit filter in
+// shared memory (32 bits per request rounded up to a power of two,
+// 1024..16384 bits, one multiplicative hash) built once per group, and a
+// binary search on a filter hit.  (Filters for rows of 3..8 requests, in
+// shared memory or in a 64-bit register, measured 40-50 % slower on the
+// whole scan: their hits diverge inside the warp.)
+constexpr uint32_t kDelCmpKeys = 8;
 constexpr uint32_t kDelFilterWords = 512;
 
 __device__ __forceinline__ uint32_t del_hash(uint32_t y, uint32_t shift) { return (y * 2654435761u) >> shift; }
@@ -642,7 +641,6 @@ __global__ void __launch_bounds__(kMutWarps * 32)
     const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint32_t g_ready = ~0u;  // group whose keys are loaded in kd / filt / sk
     uint32_t gs = 0, ge = 0, nk = 0, kd = 0, fshift = 18;
-    unsigned long long rfilt = 0;
     RowDesc d{};
     unsigned long long uhi = 0;
     uint32_t scanned = 0, scanned_cached = 0;
@@ -658,14 +656,6 @@ __global__ void __launch_bounds__(kMutWarps * 32)
             d = desc[u];
             uhi = static_cast<unsigned long long>(u) << kKeyShift;
             kd = lane < nk ? key_low(keys[gs + lane]) : 0u;
-            if (nk > kDelLaneKeys && nk <= kDelCmpKeys) {
-                // 64-bit register filter (6-bit hash) + the keys in shared memory
-                const unsigned long long bit = lane < nk ? 1ull << del_hash(kd, 26) : 0ull;
-                const uint32_t lo = __reduce_or_sync(kFull, static_cast<uint32_t>(bit));
-                const uint32_t hi = __reduce_or_sync(kFull, static_cast<uint32_t>(bit >> 32));
-                rfilt = (static_cast<unsigned long long>(hi) << 32) | lo;
-                if (lane < nk) sk[lane] = kd;
-            }
             if (nk > kDelCmpKeys) {
                 // words = nk rounded up to a power of two in [32, 512]
                 const uint32_t words = min(kDelFilterWords, max(32u, 1u << (32 - __clz(nk - 1))));
@@ -705,17 +695,7 @@ __global__ void __launch_bounds__(kMutWarps * 32)
 #pragma unroll
             for (int t = 0; t < 4; ++t)
                 if (kk + t >= d.len) e[t] = kTomb;
-            if (nk > kDelLaneKeys && nk <= kDelCmpKeys) {
-#pragma unroll
-                for (int t = 0; t < 4; ++t) {
-                    if (e[t] == kTomb || !((rfilt >> del_hash(e[t], 26)) & 1ull)) continue;
-                    for (uint32_t j = 0; j < nk; ++j)
-                        if (sk[j] == e[t]) {
-                            atomicMin(firstpos + gs + j, kk + t);
-                            break;
-                        }
-                }
-            } else if (nk <= kDelCmpKeys) {
+            if (nk <= kDelCmpKeys) {
                 int hit[4] = {-1, -1, -1, -1};
                 for (uint32_t j = 0; j < nk; ++j) {
                     const uint32_t kj = __shfl_sync(kFull, kd, j);

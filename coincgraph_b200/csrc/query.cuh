@@ -115,16 +115,69 @@ __global__ void ms_seed(const uint32_t *sources, uint32_t k, uint32_t *dist, uin
     }
 }
 
+// Direction switching of the BFS wave (Beamer, Asanovic and Patterson,
+// "Direction-optimizing breadth-first search", SC 2012, on a bitmask
+// frontier): a round runs bottom-up when the frontier holds more than
+// `on` vertices (or, once bottom-up, at least `off`); 0 disables it.
+struct MsPull {
+    AdjView rev;             // in-edges (desc null: no bottom-up)
+    uint32_t n;
+    unsigned long long full; // the wave's source bits
+    uint32_t on, off;
+};
+
+// Bottom-up round: every vertex still missing source bits ORs the frontier
+// masks of its in-neighbours (stopping once nothing is missing) and takes
+// the new bits; one thread per vertex, so `visit` needs no atomics.
+__device__ __forceinline__ void ms_bottom_up(const MsPull &pl, uint32_t *dist, uint32_t width,
+                                             unsigned long long *visit, const unsigned long long *m_in,
+                                             unsigned long long *m_out, uint32_t level, uint32_t *q_out,
+                                             uint32_t *q_cnt, uint32_t cap, Status *st, ExpandCounters &cnt) {
+    const uint32_t rounded = (pl.n + 31u) & ~31u;
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < rounded; w += gridDim.x * blockDim.x) {
+        bool want = false;
+        if (w < pl.n) {
+            const unsigned long long vis = __ldcg(visit + w);
+            const unsigned long long missing = pl.full & ~vis;
+            if (missing) {
+                const RowDesc d = pl.rev.desc[w];
+                unsigned long long acc = 0;
+                uint32_t k = 0;
+                for (; k < d.len && (acc & missing) != missing; ++k) {
+                    const uint32_t u = __ldg(pl.rev.at(d.off + k));
+                    if (u != kTomb) acc |= __ldcg(m_in + u);
+                }
+                cnt.edges += k;
+                cnt.edges_cached += k;
+                cnt.rows += d.len ? 1u : 0u;
+                const unsigned long long nb = acc & missing;
+                if (nb) {
+                    visit[w] = vis | nb;
+                    uint32_t *row = dist + static_cast<uint64_t>(w) * width;
+                    for (unsigned long long b = nb; b; b &= b - 1) row[__ffsll(static_cast<long long>(b)) - 1] = level;
+                    m_out[w] = nb;
+                    want = true;
+                    ++cnt.hits;
+                }
+            }
+        }
+        warp_enqueue(want, w, q_out, q_cnt, cap, st);
+    }
+}
+
 // Persistent multi-source closure (cooperative launch): round r expands the
 // vertices queued in round r-1 with the source bits that reached them.
-// BFS (kBfs with `visit`) is level-synchronous: round r writes depth r+1.
+// BFS (kBfs with `visit`) is level-synchronous: round r writes depth r+1,
+// top-down or (with `pl`) bottom-up.
 template <int A>
 __global__ void __launch_bounds__(kTpbMs) ms_closure(AdjView fwd, uint32_t *dist, uint32_t width,
                                                      unsigned long long *visit, MsFrontier fr, BigList big,
-                                                     uint32_t max_rounds, Status *st) {
+                                                     uint32_t max_rounds, MsPull pl, Status *st) {
     __shared__ ExpandSmem<kTpbMs, unsigned long long> sm;
     ExpandCounters cnt;
     unsigned long long src_edges = 0;
+    bool pull = false;  // every block takes the same decisions from the same counts
+    const bool can_pull = A == kBfs && visit && pl.rev.desc && pl.on;
     uint32_t r = 0;
     for (;; ++r) {
         const uint32_t n_in = ld_volatile(fr.cnt + (r % 3));
@@ -141,6 +194,17 @@ __global__ void __launch_bounds__(kTpbMs) ms_closure(AdjView fwd, uint32_t *dist
         uint32_t *out = (r & 1) ? fr.q0 : fr.q1;
         unsigned long long *m_in = (r & 1) ? fr.mask1 : fr.mask0;
         unsigned long long *m_out = (r & 1) ? fr.mask0 : fr.mask1;
+        if (can_pull) pull = n_in > (pull ? pl.off : pl.on);
+        if (pull) {
+            ms_bottom_up(pl, dist, width, visit, m_in, m_out, r + 1, out, fr.cnt + ((r + 1) % 3), fr.cap, st, cnt);
+            if (!grid_barrier(st)) break;
+            // The frontier masks were read, not taken: clear them before
+            // the next round writes into this array.
+            for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_in; i += gridDim.x * blockDim.x)
+                m_in[__ldcg(in + i)] = 0ull;
+            if (!grid_barrier(st)) break;
+            continue;
+        }
         const Defer df{big.rows, big.cnt + (r % 3), big.cap, big.split};
         for (uint32_t base = 0; base < n_in; base += gridDim.x * kTpbMs) {
             const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
@@ -170,12 +234,11 @@ __global__ void __launch_bounds__(kTpbMs) ms_closure(AdjView fwd, uint32_t *dist
         if (!grid_barrier(st)) break;
         const uint32_t nbig = min(ld_volatile(big.cnt + (r % 3)), big.cap);
         if (nbig) {
-            unsigned long long *m_out2 = m_out;
             if (A == kBfs && visit) {
-                const MsBfsOp op{dist, width, visit, m_out2, r + 1, out, fr.cnt + ((r + 1) % 3), fr.cap, st};
+                const MsBfsOp op{dist, width, visit, m_out, r + 1, out, fr.cnt + ((r + 1) % 3), fr.cap, st};
                 expand_deferred<kTpbMs, unsigned long long>(fwd, big.rows, nbig, op, cnt);
             } else {
-                const MsRelaxOp<A> op{dist, width, m_out2, out, fr.cnt + ((r + 1) % 3), fr.cap, st};
+                const MsRelaxOp<A> op{dist, width, m_out, out, fr.cnt + ((r + 1) % 3), fr.cap, st};
                 expand_deferred<kTpbMs, unsigned long long>(fwd, big.rows, nbig, op, cnt);
             }
             if (!grid_barrier(st)) break;

@@ -106,11 +106,11 @@ class TuneResult(ctypes.Structure):
         ("split_degree", ctypes.c_uint32),
         ("best_ms", ctypes.c_double),
         ("candidates", ctypes.c_uint32),
-        ("pad", ctypes.c_uint32),
+        ("pull_divisor", ctypes.c_uint32),
     ]
 
     def as_dict(self) -> dict:
-        return {name: getattr(self, name) for name, _ in self._fields_ if name != "pad"}
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 REQ_UPDATE, REQ_BFS, REQ_SSSP = 0, 1, 2

@@ -167,16 +167,19 @@ int cig_apply_batches_device(cig_handle *h, const cig_update_batch *batches, uin
 /* Launch-shape autotuner: times the static solve on the loaded graph for
  * cooperative blocks per SM in {2, 4, 8} (the frontier tile of the persistent
  * closures) x hub-row split degree in {1024, 4096, 16384} (rows at least that
- * long are expanded by the whole grid in 1024-entry chunks) and keeps the
- * fastest for the handle.  Values are unchanged (the solve's values are
+ * long are expanded by the whole grid in 1024-entry chunks), then single-
+ * source BFS waves for push/pull divisors {off, 8, 16, 32, 64} (a wave of up
+ * to 16 sources goes bottom-up while its frontier holds more than n/divisor
+ * vertices), and keeps
+ * the fastest for the handle.  Values are unchanged (the solve's values are
  * unique).  BFS/SSSP/CC.  No reference counterpart (the reference's
  * --lb_push/--lb_pull/--block_size hints have no effect). */
 typedef struct {
     uint32_t blocks_per_sm;
     uint32_t split_degree;
-    double best_ms;
+    double best_ms;           /* static solve with the chosen shape */
     uint32_t candidates;
-    uint32_t pad;
+    uint32_t pull_divisor;    /* 0: BFS waves stay top-down */
 } cig_tune_result;
 
 int cig_autotune(cig_handle *h, cig_tune_result *res);

@@ -266,7 +266,8 @@ def test_autotune_keeps_values_and_parity():
         eng.init()
         before = eng.values()
         r = eng.autotune()
-        assert r["candidates"] == 9 and r["blocks_per_sm"] in (2, 4, 8) and r["split_degree"] in (1024, 4096, 16384)
+        assert r["candidates"] == 14 and r["blocks_per_sm"] in (2, 4, 8) and r["split_degree"] in (1024, 4096, 16384)
+        assert r["pull_divisor"] in (0, 8, 16, 32, 64)
         assert np.array_equal(eng.values(), before)
         for i, b in enumerate(case.batches):
             eng.apply_batch(*b)
