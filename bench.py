@@ -70,6 +70,24 @@ def parse_args():
     return p.parse_args()
 
 
+def max_over_ranks(values, device):
+    """Replica timing: every rank's timed totals, reduced to the maximum over
+    ranks (the job is as slow as its slowest replica).  NCCL on the GPUs in
+    the bench; the same code runs over gloo on CPU in the tests."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
+def replica_value(world, steps, total_s):
+    """Whole-job batches/s of `world` independent replicas that each applied
+    `steps` batches, timed as the maximum over ranks (weak scaling)."""
+    return world * steps / total_s
+
+
 def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
@@ -377,9 +395,7 @@ def run_ours(args):
     e2e_total = sum(e2e_t)
 
     if world > 1:
-        t = torch.tensor([total_s, e2e_total], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_s, e2e_total = float(t[0]), float(t[1])
+        total_s, e2e_total = max_over_ranks([total_s, e2e_total], dev)
 
     hbm_peak, peak_kind = load_peaks()
     link_peak = link_peak_gbs(torch, dev)
@@ -424,7 +440,7 @@ def run_ours(args):
                 cpu = cpu_baseline(g, ups, args, args.warmup)
             except Exception as e:  # reported, not fatal
                 cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "port", "sample": f"failed: {e}"}
-        value = world * args.steps / total_s
+        value = replica_value(world, args.steps, total_s)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps, "higher_is_better": True,

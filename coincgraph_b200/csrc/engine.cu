@@ -510,6 +510,8 @@ struct cig_handle {
         pr64 = (opt.flags & CIG_FLAG_PR_FP64) != 0;
         if (const char *e = std::getenv("CIG_COOP_BLOCKS_PER_SM")) tune.per_sm = std::max(1, std::atoi(e));
         if (const char *e = std::getenv("CIG_SPLIT_DEG")) tune.split = std::max(32, std::atoi(e));
+        if (const char *e = std::getenv("CIG_ASYNC_PUSH")) async_push = std::atoi(e) != 0;
+        if (const char *e = std::getenv("CIG_ASYNC_PER_SM")) async_per_sm = std::max(1, std::atoi(e));
         if (const char *e = std::getenv("CIG_PULL_ON")) tune.pull_on = static_cast<uint32_t>(std::max(0, std::atoi(e)));
         if (const char *e = std::getenv("CIG_PULL_OFF")) tune.pull_off = static_cast<uint32_t>(std::max(1, std::atoi(e)));
     }
@@ -539,6 +541,8 @@ struct cig_handle {
         dfree(seg_ctl);
         dfree(state);
         dfree(qstamp);
+        dfree(ring_slot);
+        dfree(ring_ctr);
         dfree(aff_stamp);
         dfree(q0);
         dfree(q1);
@@ -835,6 +839,12 @@ struct cig_handle {
         } else {
             dmalloc(state, n);
             dmalloc(qstamp, n);
+            // vertices + chunk items of long rows (at most one chunk per kAsyncChunk arena slots)
+            ring_cap = static_cast<uint32_t>(std::min<uint64_t>(0xFFFFFFF0ull, static_cast<uint64_t>(n) + 1 +
+                                                                 fwd.seg_total * (kSegEdges / kAsyncChunk)));
+            dmalloc(ring_slot, ring_cap);
+            CK(cudaMemset(ring_slot, 0, static_cast<size_t>(ring_cap) * sizeof(unsigned long long)));
+            dmalloc(ring_ctr, kRingCtrWords);
             dmalloc(aff_stamp, n);
             dmalloc(list, n + 1);
             CK(cudaMemset(qstamp, 0, n * sizeof(uint32_t)));
@@ -917,13 +927,29 @@ struct cig_handle {
         run_push<A>();
     }
 
+    // Push closure from the queued seeds: level-synchronous (cooperative,
+    // grid barriers) for the static solve, asynchronous (ring worklist, no
+    // barriers) for the small frontiers of incremental batches.
     template <int A>
-    void run_push() {
+    void run_push(bool incremental = false) {
         const int p = prof_begin(CIG_STAGE_PUSH);
-        launch_coop(push_closure<A>, kTpb, fwd.view(), state, qstamp, tags, frontier(), big_list(), n + 2, seg_hot,
-                    status);
+        if (incremental && async_push) {
+            CK(cudaMemsetAsync(ring_ctr, 0, kRingCtrWords * sizeof(unsigned long long), stream));
+            const AsyncRing ring{ring_slot, ring_ctr, ring_cap};
+            launch(async_seed, persistent_grid(), 256, q0, small + kFr, qstamp, tags, ring, status);
+            launch(push_async<A>, sms * async_per_sm, kTpb, fwd.view(), state, qstamp, tags, ring, seg_hot, status);
+            launch(advance_tag, 1, 1, tags, 2u);
+        } else {
+            launch_coop(push_closure<A>, kTpb, fwd.view(), state, qstamp, tags, frontier(), big_list(), n + 2, seg_hot,
+                        status);
+        }
         prof_end(p);
     }
+    bool async_push = false;  // measured equal to the level-synchronous closure on RMAT (CIG_ASYNC_PUSH=1)
+    int async_per_sm = 2;  // worker blocks per SM of the asynchronous closure
+    unsigned long long *ring_slot = nullptr;  // ring_cap slots, all zero between closures
+    uint32_t ring_cap = 0;
+    unsigned long long *ring_ctr = nullptr;  // tail, head, done
 
     // ------------------------------------------------------------ PR
     template <class T>
@@ -1314,7 +1340,7 @@ struct cig_handle {
         launch(enqueue_affected<A>, persistent_grid(), 256, list, small + kAffTotal, state, frontier(), status);
         prof_end(p);
         check_launch();
-        run_push<A>();
+        run_push<A>(true);
     }
 
     template <int A>
@@ -1328,7 +1354,7 @@ struct cig_handle {
                                                                  qstamp, tags, frontier(), status);
         prof_end(p);
         check_launch();
-        run_push<A>();
+        run_push<A>(true);
     }
 
     // Copy host update arrays into the device batch buffers (pinned staging).

@@ -215,3 +215,88 @@ __device__ __forceinline__ void expand_deferred(const AdjView &view, const BigRo
 }
 
 }  // namespace cig
+
+namespace cig {
+
+// Warp-only expansion for the asynchronous closures (no block-wide tier and
+// no __syncthreads, so the warps of a block run independently): rows of 32
+// or more entries are swept by the whole warp one at a time, shorter rows
+// are gathered as in tier 3 of expand_rows.  `sm` slots [warp*32, warp*32+32)
+// belong to the calling warp.  All 32 lanes must call.
+template <int TPB, class Op, class P>
+__device__ __forceinline__ void expand_rows_warp(const AdjView &view, bool has, uint32_t x, P payload, uint64_t off,
+                                                 uint32_t deg, const Op &op, ExpandSmem<TPB, P> &sm,
+                                                 ExpandCounters &cnt) {
+    const uint32_t lane = lane_id();
+    const uint32_t warp = threadIdx.x >> 5;
+    if (has) {
+        cnt.rows += 1;
+        cnt.edges += deg;
+        if (view.cached(off)) cnt.edges_cached += deg;
+    }
+    bool med = has && deg >= 32u;
+    uint32_t mmask;
+    while ((mmask = __ballot_sync(kFull, med)) != 0u) {
+        const uint32_t leader = __ffs(mmask) - 1;
+        const uint32_t wx = __shfl_sync(kFull, x, leader);
+        const P wp = __shfl_sync(kFull, payload, leader);
+        const uint32_t wdeg = __shfl_sync(kFull, deg, leader);
+        const uint64_t woff = __shfl_sync(kFull, static_cast<unsigned long long>(off), leader);
+        if (lane == leader) med = false;
+        if (wdeg <= kSegEdges) {
+            const uint32_t *rp = view.at(woff);  // a block of <= 2^14 slots lies in one segment
+            for (uint32_t base = 0; base < wdeg; base += 32u) {
+                const uint32_t k = base + lane;
+                const bool valid = k < wdeg;
+                const uint32_t y = valid ? __ldg(rp + k) : 0u;
+                cnt.hits += op.edge(valid && y != kTomb, wx, wp, y);
+            }
+        } else {
+            for (uint32_t base = 0; base < wdeg; base += 32u) {
+                const uint32_t k = base + lane;
+                const bool valid = k < wdeg;
+                const uint32_t y = valid ? __ldg(view.at(woff + k)) : 0u;
+                cnt.hits += op.edge(valid && y != kTomb, wx, wp, y);
+            }
+        }
+    }
+    const uint32_t mydeg = (has && deg < 32u) ? deg : 0u;
+    uint32_t incl = mydeg;
+#pragma unroll
+    for (uint32_t o = 1; o < 32u; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    if (total == 0) return;
+    const uint32_t wb = warp * 32u;
+    __syncwarp();
+    sm.f_scan[wb + lane] = incl - mydeg;
+    sm.f_x[wb + lane] = x;
+    sm.f_payload[wb + lane] = payload;
+    sm.f_ptr[wb + lane] = mydeg ? view.at(off) : nullptr;
+    __syncwarp();
+    for (uint32_t base = 0; base < total; base += 32u) {
+        const uint32_t e = base + lane;
+        const bool valid = e < total;
+        uint32_t ox = 0, y = 0;
+        P op_ = 0;
+        if (valid) {
+            uint32_t lo = 0, hi = 32;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (sm.f_scan[wb + mid] <= e)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            ox = sm.f_x[wb + lo];
+            op_ = sm.f_payload[wb + lo];
+            y = __ldg(sm.f_ptr[wb + lo] + (e - sm.f_scan[wb + lo]));
+        }
+        cnt.hits += op.edge(valid && y != kTomb, ox, op_, y);
+    }
+    __syncwarp();
+}
+
+}  // namespace cig

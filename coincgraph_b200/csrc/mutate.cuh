@@ -765,21 +765,29 @@ __global__ void del_finish(const RowDesc *desc, const unsigned long long *keys, 
                            const uint32_t *firstpos, uint32_t *compact, uint32_t *compact_count,
                            unsigned long long *stats) {
     const uint32_t ng = *gr.count;
-    unsigned long long changed = 0;
-    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
-        if (!chunks[g]) continue;  // ordered group, or empty row
-        const uint32_t gs = gr.start[g];
-        const uint32_t ge = gr.end[g];
-        bool any = false;
-        for (uint32_t i = gs; i < ge && !any; ++i) any = firstpos[i] != kInf;
-        if (!any) continue;
-        ++changed;
-        const uint32_t u = key_src(keys[gs]);
-        const RowDesc d = desc[u];
-        const uint32_t tombs = rd_tombs(d);
-        if (4ull * tombs >= d.len || tombs >= kMaxTombs / 2) compact[atomicAdd(compact_count, 1u)] = u;
+    const uint32_t rounded = (ng + 31u) & ~31u;
+    uint32_t changed = 0;
+    // Warp-aggregated appends and counts: ~10^5 rows per batch would
+    // otherwise queue on one counter address.
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < rounded; g += gridDim.x * blockDim.x) {
+        bool want = false;
+        uint32_t u = 0;
+        if (g < ng && chunks[g]) {  // flat group (ordered groups and empty rows have no chunks)
+            const uint32_t gs = gr.start[g];
+            const uint32_t ge = gr.end[g];
+            bool any = false;
+            for (uint32_t i = gs; i < ge && !any; ++i) any = firstpos[i] != kInf;
+            if (any) {
+                ++changed;
+                u = key_src(keys[gs]);
+                const RowDesc d = desc[u];
+                const uint32_t tombs = rd_tombs(d);
+                want = 4ull * tombs >= d.len || tombs >= kMaxTombs / 2;
+            }
+        }
+        warp_enqueue(want, u, compact, compact_count, 0xFFFFFFFFu, nullptr);
     }
-    if (stats && changed) atomicAdd(&stats[kCntChanged], changed);
+    if (stats) warp_count(&stats[kCntChanged], changed);
 }
 
 // ---------------------------------------------------------------- compaction
@@ -842,21 +850,37 @@ __global__ void __launch_bounds__(kTpbMut) compact_rows(AdjView view, RowDesc *d
 __global__ void plan_add(const RowDesc *desc, const unsigned long long *keys, Groups gr, unsigned long long *plan,
                          ArenaAlloc *al) {
     const uint32_t ng = *gr.count;
-    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
-        const uint32_t gs = gr.start[g];
-        const uint32_t ge = gr.end[g];
-        const RowDesc d = desc[key_src(keys[gs])];
-        const unsigned long long used = static_cast<unsigned long long>(d.len) + (ge - gs);
-        const unsigned long long live = static_cast<unsigned long long>(rd_live(d)) + (ge - gs);
+    const uint32_t rounded = (ng + 31u) & ~31u;
+    const uint32_t lane = lane_id();
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < rounded; g += gridDim.x * blockDim.x) {
         unsigned long long p = kKeyNone;
-        if (live > 0xFFFFFFFFull) {
-            p = kKeyNone - 1;  // degree overflow, reported by the apply kernel
-        } else if (rd_cls(d) == 0 || used > (1ull << rd_cls(d))) {
-            const uint32_t cls = class_for(static_cast<uint32_t>(live));
-            const uint32_t rank = atomicAdd(&al->demand[cls], 1u);
-            p = (static_cast<unsigned long long>(cls) << 32) | rank;
+        bool move = false;
+        uint32_t cls = 0;
+        if (g < ng) {
+            const uint32_t gs = gr.start[g];
+            const uint32_t ge = gr.end[g];
+            const RowDesc d = desc[key_src(keys[gs])];
+            const unsigned long long used = static_cast<unsigned long long>(d.len) + (ge - gs);
+            const unsigned long long live = static_cast<unsigned long long>(rd_live(d)) + (ge - gs);
+            if (live > 0xFFFFFFFFull) {
+                p = kKeyNone - 1;  // degree overflow, reported by the apply kernel
+            } else if (rd_cls(d) == 0 || used > (1ull << rd_cls(d))) {
+                cls = class_for(static_cast<uint32_t>(live));
+                move = true;
+            }
         }
-        plan[g] = p;
+        // Ranks within a class, one atomic per class present in the warp
+        // (tens of thousands of moving rows share a handful of classes).
+        const uint32_t movers = __ballot_sync(kFull, move);
+        if (move) {
+            const uint32_t peers = __match_any_sync(movers, cls);
+            const uint32_t leader = __ffs(peers) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(&al->demand[cls], static_cast<uint32_t>(__popc(peers)));
+            base = __shfl_sync(peers, base, leader);
+            p = (static_cast<unsigned long long>(cls) << 32) | (base + __popc(peers & lanemask_lt()));
+        }
+        if (g < ng) plan[g] = p;
     }
 }
 
