@@ -464,7 +464,8 @@ def run_ours(args):
             "gpu_launches": launches,
             "mean_batch": {k: float(np.mean([s[k] for s in stats])) for k in
                            ("affected", "seeds", "rounds", "edges_scanned", "edges_scanned_cached",
-                            "changed_sources", "relocated_rows", "missing_deletes")},
+                            "changed_sources", "relocated_rows", "missing_deletes", "cache_segments_loaded",
+                            "cache_segments_evicted")},
         }
         print(json.dumps(line), flush=True)
     eng.close()

@@ -25,7 +25,7 @@
 namespace cig {
 
 constexpr uint32_t kAdmitScore = 8192;   // default: ~half a segment of entries read recently
-constexpr uint32_t kColdScore = 256;     // default: evictable below this
+constexpr uint32_t kColdScore = 2048;    // default: evictable below this (256, 2048, 8192 measured within 2 %)
 constexpr uint32_t kMaxAdmit = 64;       // admissions per batch (4 MiB over the host link)
 constexpr uint32_t kMaxEvict = 1024;     // evictions per batch
 constexpr uint32_t kNewScore = 16384;    // score of a freshly allocated segment

@@ -218,21 +218,29 @@ __device__ __forceinline__ void expand_deferred(const AdjView &view, const BigRo
 
 namespace cig {
 
-// Warp-only expansion for the asynchronous closures (no block-wide tier and
-// no __syncthreads, so the warps of a block run independently): rows of 32
-// or more entries are swept by the whole warp one at a time, shorter rows
-// are gathered as in tier 3 of expand_rows.  `sm` slots [warp*32, warp*32+32)
-// belong to the calling warp.  All 32 lanes must call.
+// Warp-only expansion (no block-wide tier and no __syncthreads, so the warps
+// of a block run independently): rows of 32 or more entries are swept by the
+// whole warp one at a time, shorter rows are gathered as in tier 3 of
+// expand_rows; rows of at least `defer.split` entries go to the deferred
+// list as in expand_rows.  `sm` slots [warp*32, warp*32+32) belong to the
+// calling warp.  All 32 lanes must call.
 template <int TPB, class Op, class P>
 __device__ __forceinline__ void expand_rows_warp(const AdjView &view, bool has, uint32_t x, P payload, uint64_t off,
                                                  uint32_t deg, const Op &op, ExpandSmem<TPB, P> &sm,
-                                                 ExpandCounters &cnt) {
+                                                 ExpandCounters &cnt, const Defer &defer = Defer{nullptr, nullptr, 0, 0}) {
     const uint32_t lane = lane_id();
     const uint32_t warp = threadIdx.x >> 5;
     if (has) {
         cnt.rows += 1;
         cnt.edges += deg;
         if (view.cached(off)) cnt.edges_cached += deg;
+    }
+    if (has && defer.rows && deg >= defer.split) {
+        const uint32_t i = atomicAdd(defer.count, 1u);
+        if (i < defer.cap) {
+            defer.rows[i] = BigRow{off, static_cast<unsigned long long>(payload), x, deg};
+            has = false;
+        }
     }
     bool med = has && deg >= 32u;
     uint32_t mmask;

@@ -223,6 +223,8 @@ __global__ void __launch_bounds__(kTpbMs) ms_closure(AdjView fwd, uint32_t *dist
                 has = m != 0ull && deg > 0;
                 if (has) src_edges += static_cast<unsigned long long>(__popcll(m)) * deg;
             }
+            // (Warp-only tiers, expand_rows_warp, measured the same for BFS and
+            // 12 % slower for SSSP waves than the block tiers.)
             if (A == kBfs && visit) {
                 const MsBfsOp op{dist, width, visit, m_out, r + 1, out, fr.cnt + ((r + 1) % 3), fr.cap, st};
                 expand_rows<kTpbMs>(fwd, has, x, m, off, deg, op, sm, cnt, df);
