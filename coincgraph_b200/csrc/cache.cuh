@@ -9,7 +9,8 @@
 //     segment; the service folds it into a decayed `score` (score/2 + hot);
 //   - new segments handed out by the block allocator take a free slot at
 //     once (their rows were just written, so they are hot), and the service
-//     keeps `reserve` slots free for them by evicting cold segments;
+//     keeps `reserve` slots free for them by evicting the coldest resident
+//     segments (a histogram of log2(score) picks the threshold);
 //   - host segments whose score passed admit_score are copied in, at most
 //     kMaxAdmit per batch, into slots freed from cold segments;
 //   - an evicted segment is written back first if it is dirty.
@@ -25,7 +26,8 @@
 namespace cig {
 
 constexpr uint32_t kAdmitScore = 8192;   // default: ~half a segment of entries read recently
-constexpr uint32_t kColdScore = 2048;    // default: evictable below this (256, 2048, 8192 measured within 2 %)
+constexpr uint32_t kColdScore = 1u << 30;  // default cap: segments scoring this much are never evicted
+constexpr int kScoreBuckets = 33;          // bucket of a score: 32 - clz(score)
 constexpr uint32_t kMaxAdmit = 64;       // admissions per batch (4 MiB over the host link)
 constexpr uint32_t kMaxEvict = 1024;     // evictions per batch
 constexpr uint32_t kNewScore = 16384;    // score of a freshly allocated segment
@@ -38,7 +40,11 @@ enum SegCtl : int {
     kCtlAdmits = 4,     // hot host segments found this service
     kCtlEvictNeed = 5,  // evictions this service
     kCtlReserve = 6,    // free slots kept for new segments
-    kCtlCount = 8
+    kCtlThreshold = 7,  // victims: bucket below this ...
+    kCtlExtra = 8,      // ... plus this many from the threshold bucket
+    kCtlExtraTaken = 9,
+    kCtlHist = 16,      // kScoreBuckets counters of resident scores
+    kCtlCount = 16 + kScoreBuckets
 };
 
 struct SegTable {
@@ -82,29 +88,34 @@ __global__ void seg_assign_new(SegTable t, const unsigned long long *seg_bump, S
     t.ctl[kCtlBumpSeen] = max(seen, bump);
 }
 
-// Decay scores, pick eviction victims among cold resident segments and
-// admission candidates among hot host segments.  Grid-stride over segments.
-__global__ void seg_rescore(SegTable t, uint32_t bump, uint32_t want_victims) {
+__device__ __forceinline__ uint32_t score_bucket(uint32_t sc) { return 32u - __clz(sc); }
+
+// Decay scores, histogram the resident ones (evictable: below cold_score)
+// and list admission candidates among hot host segments.  Grid-stride.
+__global__ void seg_rescore(SegTable t, uint32_t bump) {
+    __shared__ uint32_t hist[kScoreBuckets];
+    for (uint32_t b = threadIdx.x; b < kScoreBuckets; b += blockDim.x) hist[b] = 0;
+    __syncthreads();
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < bump; s += gridDim.x * blockDim.x) {
         const uint32_t h = t.hot[s];
         if (h) t.hot[s] = 0;
         const uint32_t sc = (t.score[s] >> 1) + min(h, 1u << 24);
         t.score[s] = sc;
-        const int32_t slot = t.seg_slot[s];
-        if (slot >= 0) {
-            if (sc < t.cold_score && want_victims) {
-                const uint32_t i = atomicAdd(t.ctl + kCtlVictims, 1u);
-                if (i < want_victims) t.victims[i] = static_cast<uint32_t>(slot);
-            }
+        if (t.seg_slot[s] >= 0) {
+            if (sc < t.cold_score) atomicAdd(hist + score_bucket(sc), 1u);
         } else if (sc >= t.admit_score) {
             const uint32_t i = atomicAdd(t.ctl + kCtlAdmits, 1u);
             if (i < kMaxAdmit) t.admits[i] = s;
         }
     }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < kScoreBuckets; b += blockDim.x)
+        if (hist[b]) atomicAdd(t.ctl + kCtlHist + b, hist[b]);
 }
 
-// How many victims to evict: enough to keep `reserve` slots free for new
-// segments (twice the last batches' count, 16..1024) plus the admissions.
+// How many to evict: enough to keep `reserve` slots free for new segments
+// (twice the last batches' count, 16..1024) plus the admissions; the
+// coldest first: whole buckets below a threshold, then part of it.
 __global__ void seg_plan(SegTable t) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     const uint32_t reserve = min(1024u, max(16u, 2u * t.ctl[kCtlNewLast]));
@@ -112,13 +123,42 @@ __global__ void seg_plan(SegTable t) {
     t.ctl[kCtlReserve] = reserve;
     const uint32_t want = reserve + min(t.ctl[kCtlAdmits], kMaxAdmit);
     const uint32_t top = t.ctl[kCtlFreeTop];
-    const uint32_t need = want > top ? want - top : 0u;
-    t.ctl[kCtlEvictNeed] = min(need, min(t.ctl[kCtlVictims], kMaxEvict));
+    uint32_t need = min(want > top ? want - top : 0u, kMaxEvict);
+    uint32_t below = 0, b = 0;
+    for (; b < static_cast<uint32_t>(kScoreBuckets); ++b) {
+        const uint32_t c = t.ctl[kCtlHist + b];
+        if (below + c >= need) break;
+        below += c;
+    }
+    if (b == static_cast<uint32_t>(kScoreBuckets)) need = below;  // fewer evictable segments than wanted
+    t.ctl[kCtlThreshold] = b;
+    t.ctl[kCtlExtra] = need - below;
+    t.ctl[kCtlExtraTaken] = 0;
+    t.ctl[kCtlEvictNeed] = need;
+}
+
+// The victims chosen by seg_plan.  Grid-stride over segments.
+__global__ void seg_pick(SegTable t, uint32_t bump) {
+    const uint32_t thr = t.ctl[kCtlThreshold], extra = t.ctl[kCtlExtra], need = t.ctl[kCtlEvictNeed];
+    if (!need) return;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < bump; s += gridDim.x * blockDim.x) {
+        const int32_t slot = t.seg_slot[s];
+        if (slot < 0) continue;
+        const uint32_t sc = t.score[s];
+        if (sc >= t.cold_score) continue;
+        const uint32_t b = score_bucket(sc);
+        bool take = b < thr;
+        if (!take && b == thr && extra) take = atomicAdd(t.ctl + kCtlExtraTaken, 1u) < extra;
+        if (take) {
+            const uint32_t i = atomicAdd(t.ctl + kCtlVictims, 1u);
+            if (i < need) t.victims[i] = static_cast<uint32_t>(slot);
+        }
+    }
 }
 
 // One block per victim slot: write back if dirty, unmap, free the slot.
 __global__ void seg_evict(SegTable t, const uint32_t *cache, uint32_t *host, Status *st) {
-    const uint32_t nv = t.ctl[kCtlEvictNeed];
+    const uint32_t nv = min(t.ctl[kCtlEvictNeed], t.ctl[kCtlVictims]);
     for (uint32_t v = blockIdx.x; v < nv; v += gridDim.x) {
         const uint32_t slot = t.victims[v];
         const int32_t seg = t.slot_seg[slot];

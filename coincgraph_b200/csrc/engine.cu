@@ -1136,8 +1136,10 @@ struct cig_handle {
         if (!refresh) return;
         const SegTable t = seg_table();
         CK(cudaMemsetAsync(seg_ctl + kCtlVictims, 0, 2 * sizeof(uint32_t), stream));
-        launch(seg_rescore, grid_for(fwd.seg_total), 256, t, static_cast<uint32_t>(fwd.seg_total), kMaxEvict);
+        CK(cudaMemsetAsync(seg_ctl + kCtlHist, 0, kScoreBuckets * sizeof(uint32_t), stream));
+        launch(seg_rescore, grid_for(fwd.seg_total), 256, t, static_cast<uint32_t>(fwd.seg_total));
         launch(seg_plan, 1, 32, t);
+        launch(seg_pick, grid_for(fwd.seg_total), 256, t, static_cast<uint32_t>(fwd.seg_total));
         launch(seg_evict, static_cast<int>(std::min<uint64_t>(kMaxEvict, sms * 4)), 256, t, fwd.dev, fwd.host_dptr,
                status);
         launch(seg_admit, static_cast<int>(kMaxAdmit), 256, t, fwd.dev, fwd.host_dptr, status);
