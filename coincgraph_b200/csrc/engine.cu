@@ -186,9 +186,11 @@ enum SmallIdx : int {
     kBigRows = 13,  // 3 counters of deferred hub rows
     kCompactCount = 16,
     kOrderedCount = 17,
+    kIndexedCount = 20,  // deletion groups answered by the position index
+    kIdxRows = 21,       // rows of an arena being indexed (load time)
     kGaF = 18,  // addition-phase group counts of a presorted batch
     kGaR = 19,
-    kSmallCount = 20
+    kSmallCount = 24
 };
 
 constexpr uint32_t kBigRowCap = 65536;
@@ -292,6 +294,76 @@ struct cig_handle {
     // groups left to the ordered kernels, first match per key
     uint32_t *chunks = nullptr, *chunk_end = nullptr, *ordered = nullptr, *firstpos = nullptr;
     uint32_t *chunk_map = nullptr;  // group of every 512-entry scan chunk
+    uint8_t *gtype = nullptr;             // kind of every deletion group
+    uint32_t *indexed_groups = nullptr;   // deletion groups of indexed rows
+
+    // Position index of hub rows, per arena (posindex.cuh); off with
+    // CIG_POS_INDEX=0 or when the tables would not fit their share of memory.
+    struct IndexBuf {
+        unsigned long long *keys = nullptr;
+        uint2 *val = nullptr;
+        uint32_t *rowbit = nullptr;
+        uint64_t cap = 0;
+        uint64_t rows = 0, entries = 0;  // at the last build
+        uint64_t inserted = 0;           // addition requests since (a bound on new keys)
+        uint64_t builds = 0;
+    } ixb[2];  // [0] forward, [1] reverse
+    bool use_index = true;
+    uint32_t index_cls = kIdxCls;             // smallest block class indexed
+    uint64_t index_headroom = 1ull << 20;    // table slots beyond twice the entries
+    PosIndex pos_index(bool forward) const {
+        const IndexBuf &b = ixb[forward ? 0 : 1];
+        return PosIndex{b.keys, b.val, b.cap ? b.cap - 1 : 0, b.rowbit};
+    }
+
+    // (Re)build the index of arena A: the rows of class >= index_cls now, a
+    // table of at least twice their slots plus index_headroom (so that appends do not
+    // fill it), if it fits a quarter of the free device memory; otherwise the
+    // arena goes unindexed.  Deleted keys keep their slots until a rebuild,
+    // which mutate_add_arena asks for when the keys inserted since the last
+    // build could take the load factor past one half.  Synchronises.
+    void build_index(DevArena &A, bool forward) {
+        IndexBuf &b = ixb[forward ? 0 : 1];
+        if (!use_index) return;
+        CK(cudaMemsetAsync(small64 + 2, 0, sizeof(unsigned long long), stream));
+        launch(idx_count_slots, persistent_grid(), 256, A.desc, n, index_cls, small64 + 2);
+        unsigned long long entries = 0;
+        CK(cudaMemcpyAsync(&entries, small64 + 2, sizeof(entries), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        uint64_t cap = 1;
+        while (cap < 2 * entries + index_headroom) cap <<= 1;
+        if (cap > b.cap) {
+            dfree(b.keys);
+            dfree(b.val);
+            b.cap = 0;
+            size_t fr = 0, tot = 0;
+            CK(cudaMemGetInfo(&fr, &tot));
+            if (entries == 0 || cap * (sizeof(unsigned long long) + sizeof(uint2)) > fr / 4) {
+                dfree(b.rowbit);
+                b = IndexBuf{};
+                return;
+            }
+            dmalloc(b.keys, cap);
+            dmalloc(b.val, cap);
+            b.cap = cap;
+        }
+        const uint32_t words = (n + 31) / 32;
+        if (!b.rowbit) dmalloc(b.rowbit, words);
+        b.entries = entries;
+        b.inserted = 0;
+        b.builds += 1;
+        const PosIndex ix = pos_index(forward);
+        launch(idx_init, sms * 8, 256, ix);
+        CK(cudaMemsetAsync(small + kIdxRows, 0, sizeof(uint32_t), stream));
+        launch(idx_pick_rows, persistent_grid(), 256, A.desc, n, index_cls, b.rowbit, tmp_u32, small + kIdxRows, n,
+               status);
+        launch(idx_build, sms * 4, 256, A.view(), A.desc, tmp_u32, small + kIdxRows, ix, status);
+        check_launch();
+        uint32_t rows = 0;
+        CK(cudaMemcpyAsync(&rows, small + kIdxRows, sizeof(rows), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        b.rows = rows;
+    }
     uint64_t chunk_map_cap = 0;
     int del_scan_per_sm = 0;
     int del_scan_blocks_per_sm() {
@@ -511,6 +583,10 @@ struct cig_handle {
         if (const char *e = std::getenv("CIG_COOP_BLOCKS_PER_SM")) tune.per_sm = std::max(1, std::atoi(e));
         if (const char *e = std::getenv("CIG_SPLIT_DEG")) tune.split = std::max(32, std::atoi(e));
         if (const char *e = std::getenv("CIG_ASYNC_PUSH")) async_push = std::atoi(e) != 0;
+        if (const char *e = std::getenv("CIG_POS_INDEX")) use_index = std::atoi(e) != 0;
+        if (const char *e = std::getenv("CIG_POS_INDEX_CLS")) index_cls = static_cast<uint32_t>(std::atoi(e));
+        if (const char *e = std::getenv("CIG_POS_INDEX_HEADROOM"))
+            index_headroom = std::max<uint64_t>(64, std::strtoull(e, nullptr, 10));
         if (const char *e = std::getenv("CIG_ASYNC_PER_SM")) async_per_sm = std::max(1, std::atoi(e));
         if (const char *e = std::getenv("CIG_PULL_ON")) tune.pull_on = static_cast<uint32_t>(std::max(0, std::atoi(e)));
         if (const char *e = std::getenv("CIG_PULL_OFF")) tune.pull_off = static_cast<uint32_t>(std::max(1, std::atoi(e)));
@@ -566,6 +642,12 @@ struct cig_handle {
         free_batch();
         dfree(tmp_u32);
         dfree(chunk_map);
+        for (auto &b : ixb) {
+            dfree(b.keys);
+            dfree(b.val);
+            dfree(b.rowbit);
+            b = IndexBuf{};
+        }
         dfree(bsnap);
         dfree(bdig);
         for (auto &e : bev) cudaEventDestroy(e);
@@ -589,6 +671,8 @@ struct cig_handle {
         dfree(mr);
         dfree(bigf);
         dfree(bigr);
+        dfree(gtype);
+        dfree(indexed_groups);
         dfree(kc);
         dfree(tc);
         dfree(gaf);
@@ -640,6 +724,8 @@ struct cig_handle {
         dmalloc(chunks, cap);
         dmalloc(chunk_end, cap);
         dmalloc(ordered, cap);
+        dmalloc(gtype, cap);
+        dmalloc(indexed_groups, cap);
         dmalloc(firstpos, cap);
         dmalloc(gflags, 4 * cap);
         dmalloc(gpos, 4 * cap);
@@ -798,6 +884,8 @@ struct cig_handle {
         dmalloc(q0, n + 1);
         dmalloc(q1, n + 1);
         dmalloc(tmp_u32, n);
+        build_index(fwd, true);
+        if (opt.algo != CIG_PR) build_index(rev, false);
         if (opt.algo == CIG_PR) {
             const size_t es = pr64 ? sizeof(double) : sizeof(float);
             CK(cudaMalloc(&pr_rank, n * es));
@@ -1242,7 +1330,11 @@ struct cig_handle {
         CK(cudaMemsetAsync(chunks, 0, nd * sizeof(uint32_t), stream));
         CK(cudaMemsetAsync(firstpos, 0xFF, nd * sizeof(uint32_t), stream));
         // Flat path: rows whose deletion requests are all distinct.
-        launch(del_classify, persistent_grid(), 256, A.desc, sorted, grp, chunks, ordered, ocount);
+        uint32_t *icount = small + kIndexedCount;
+        CK(cudaMemsetAsync(icount, 0, sizeof(uint32_t), stream));
+        const PosIndex ix = pos_index(forward);
+        launch(del_classify, persistent_grid(), 256, A.desc, sorted, grp, chunks, gtype, ordered, ocount, ix,
+               indexed_groups, icount);
         {
             size_t bytes = cub_bytes;
             CK(cub::DeviceScan::InclusiveSum(cub, bytes, chunks, chunk_end, static_cast<int>(nd), stream));
@@ -1261,16 +1353,21 @@ struct cig_handle {
         const int ps = prof_begin(CIG_STAGE_DEL_SCAN);
         launch(del_scan, sms * del_scan_blocks_per_sm(), kMutWarps * 32, A.view(), A.desc, sorted, grp, chunk_end,
                chunk_map, m, firstpos, status->counters, forward ? seg_hot : nullptr);
+        if (ix.keys)
+            launch(del_index, persistent_grid(), 256, A.view(), A.desc, sorted, grp, indexed_groups, icount, firstpos,
+                   ix, status);
         prof_end(ps);
         if (prof_on) prof[CIG_STAGE_DEL_SCAN].hits += nd;
         launch(del_apply, grid_for(nd), 256, A.view(), A.desc, sorted, m, firstpos, stats);
-        launch(del_finish, persistent_grid(), 256, A.desc, sorted, grp, chunks, firstpos, compact, ccount, stats);
+        launch(del_finish, persistent_grid(), 256, A.desc, sorted, grp, gtype, firstpos, compact, ccount, stats);
         // Ordered path: rows with repeated requests for a destination.
         launch(mutate_delete, persistent_grid(), kMutWarps * 32, A.view(), A.desc, sorted, grp, ordered, ocount,
                matched, big, bcount, compact, ccount, stats, status);
         launch(mutate_delete_big, sms * 4, kTpbMut, A.view(), A.desc, sorted, grp, big, bcount, matched, compact,
                ccount, stats, status);
-        launch(compact_rows, sms * 4, kTpbMut, A.view(), A.desc, compact, ccount);
+        if (ix.keys) launch(idx_fix_ordered, persistent_grid(), 256, A.view(), A.desc, sorted, grp, ordered, ocount, ix,
+                            status);
+        launch(compact_rows, sms * 4, kTpbMut, A.view(), A.desc, compact, ccount, ix, status);
         prof_end(p);
         check_launch();
     }
@@ -1303,15 +1400,21 @@ struct cig_handle {
         CK(cudaMemsetAsync(bcount, 0, sizeof(uint32_t), stream));
         prof_end(p);
         p = prof_begin(forward ? CIG_STAGE_ADD : CIG_STAGE_ADD_REV);
+        if (ixb[forward ? 0 : 1].cap) {
+            IndexBuf &b = ixb[forward ? 0 : 1];
+            b.inserted += na;
+            if (2 * (b.entries + b.inserted) > b.cap) build_index(A, forward);
+        }
         launch(plan_add, persistent_grid(), 256, A.desc, sorted, grp, plan, A.alloc);
         launch(alloc_classes, 1, 64, A.alloc, status);
         if (forward && refresh) launch(seg_assign_new, 1, 32, seg_table(), &A.alloc->seg_bump, status);
         unsigned long long *stats = with_stats ? status->counters : nullptr;
         const uint32_t *vals = forward ? d_av : d_au;
+        const PosIndex ix = pos_index(forward);
         launch(mutate_add, persistent_grid(), 256, A.view(), A.desc, sorted, grp, plan, A.alloc, vals, big, bcount,
-               stats, status);
+               stats, ix, status);
         launch(mutate_add_big, sms * 2, kTpbMut, A.view(), A.desc, sorted, grp, plan, A.alloc, vals, big, bcount,
-               stats, status);
+               stats, ix, status);
         prof_end(p);
         check_launch();
     }

@@ -28,6 +28,7 @@
 #include <cub/block/block_scan.cuh>
 
 #include "common.cuh"
+#include "posindex.cuh"
 
 namespace cig {
 
@@ -577,19 +578,95 @@ constexpr uint32_t kSmemKeys = 256;
 
 // Classify groups: chunk count for flat rows, ordered list for the rest.
 // `chunks` must be zero beyond the group count (it is scanned whole).
+// Kinds of deletion groups: rows with repeated requests take the ordered
+// kernels; rows with distinct requests the flat scan, or the position index
+// when the row is indexed (posindex.cuh).
+enum : uint8_t { kGroupOrdered = 0, kGroupChunked = 1, kGroupIndexed = 2 };
+
 __global__ void del_classify(const RowDesc *desc, const unsigned long long *keys, Groups gr, uint32_t *chunks,
-                             uint32_t *ordered, uint32_t *ordered_count) {
+                             uint8_t *gtype, uint32_t *ordered, uint32_t *ordered_count, PosIndex ix,
+                             uint32_t *indexed, uint32_t *indexed_count) {
     const uint32_t ng = *gr.count;
-    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+    const uint32_t rounded = (ng + 31u) & ~31u;
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < rounded; g += gridDim.x * blockDim.x) {
+        bool dup = false, by_index = false;
+        if (g < ng) {
+            const uint32_t gs = gr.start[g];
+            const uint32_t ge = gr.end[g];
+            for (uint32_t i = gs; i + 1 < ge && !dup; ++i) dup = keys[i] == keys[i + 1];
+            const uint32_t u = key_src(keys[gs]);
+            by_index = !dup && idx_row(ix, u);
+            gtype[g] = dup ? kGroupOrdered : by_index ? kGroupIndexed : kGroupChunked;
+            chunks[g] = (dup || by_index) ? 0u : (desc[u].len + kDelChunk - 1) / kDelChunk;
+        }
+        warp_enqueue(dup, g, ordered, ordered_count, 0xFFFFFFFFu, nullptr);
+        warp_enqueue(by_index, g, indexed, indexed_count, 0xFFFFFFFFu, nullptr);
+    }
+}
+
+// Indexed rows with distinct requests: the first live position of every key
+// from the index (one warp per group, lanes over its keys); the entry loses
+// one occurrence and, when more remain, moves to the next one (a scan from
+// the deleted position on, rare: parallel edges).
+__global__ void del_index(AdjView view, const RowDesc *desc, const unsigned long long *keys, Groups gr,
+                          const uint32_t *list, const uint32_t *count, uint32_t *firstpos, PosIndex ix, Status *st) {
+    const uint32_t lane = lane_id();
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t nl = *count;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nl; i += warps) {
+        const uint32_t g = list[i];
+        const uint32_t gs = gr.start[g];
+        const uint32_t nk = gr.end[g] - gs;
+        const uint32_t u = key_src(keys[gs]);
+        const RowDesc d = desc[u];
+        for (uint32_t j = lane; j < nk; j += 32u) {
+            const uint32_t v = key_low(keys[gs + j]);
+            const unsigned long long s = idx_find(ix, (static_cast<unsigned long long>(u) << 32) | v);
+            if (s == ~0ull) continue;  // not in the row: a missing delete
+            const uint2 e = ix.val[s];
+            if (e.y == 0u || e.x >= d.len) {
+                if (e.y != 0u) set_error(st, kErrInternal, 0x1d2u);
+                continue;
+            }
+            firstpos[gs + j] = e.x;
+            if (e.y == 1u) {
+                ix.val[s] = make_uint2(kInf, 0u);
+                ix.keys[s] = kIdxDeleted;
+            } else {
+                uint32_t q = e.x + 1;
+                while (q < d.len && *view.at(d.off + q) != v) ++q;
+                if (q >= d.len) set_error(st, kErrInternal, 0x1d3u);
+                ix.val[s] = make_uint2(q < d.len ? q : kInf, e.y - 1u);
+            }
+        }
+    }
+}
+
+// After the ordered kernels: the entries of every key of an ordered group on
+// an indexed row are recounted from the row (rare: repeated requests).
+__global__ void idx_fix_ordered(AdjView view, const RowDesc *desc, const unsigned long long *keys, Groups gr,
+                                const uint32_t *ordered, const uint32_t *ordered_count, PosIndex ix, Status *st) {
+    const uint32_t no = *ordered_count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < no; i += gridDim.x * blockDim.x) {
+        const uint32_t g = ordered[i];
         const uint32_t gs = gr.start[g];
         const uint32_t ge = gr.end[g];
-        bool dup = false;
-        for (uint32_t i = gs; i + 1 < ge && !dup; ++i) dup = keys[i] == keys[i + 1];
-        if (dup) {
-            ordered[atomicAdd(ordered_count, 1u)] = g;
-            chunks[g] = 0;
-        } else {
-            chunks[g] = (desc[key_src(keys[gs])].len + kDelChunk - 1) / kDelChunk;
+        const uint32_t u = key_src(keys[gs]);
+        if (!idx_row(ix, u)) continue;
+        const RowDesc d = desc[u];
+        for (uint32_t j = gs; j < ge; ++j) {
+            if (j > gs && keys[j] == keys[j - 1]) continue;  // one pass per distinct key
+            const uint32_t v = key_low(keys[j]);
+            const unsigned long long s = idx_find(ix, (static_cast<unsigned long long>(u) << 32) | v);
+            if (s == ~0ull) continue;
+            uint32_t first = kInf, live = 0;
+            for (uint32_t q = 0; q < d.len; ++q)
+                if (*view.at(d.off + q) == v) {
+                    if (first == kInf) first = q;
+                    ++live;
+                }
+            ix.val[s] = make_uint2(first, live);
+            if (!live) ix.keys[s] = kIdxDeleted;
         }
     }
 }
@@ -761,7 +838,7 @@ __global__ void del_apply(AdjView view, RowDesc *desc, const unsigned long long 
 }
 
 // Queue flat rows whose tombstones reached a quarter of their length.
-__global__ void del_finish(const RowDesc *desc, const unsigned long long *keys, Groups gr, const uint32_t *chunks,
+__global__ void del_finish(const RowDesc *desc, const unsigned long long *keys, Groups gr, const uint8_t *gtype,
                            const uint32_t *firstpos, uint32_t *compact, uint32_t *compact_count,
                            unsigned long long *stats) {
     const uint32_t ng = *gr.count;
@@ -772,7 +849,7 @@ __global__ void del_finish(const RowDesc *desc, const unsigned long long *keys, 
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < rounded; g += gridDim.x * blockDim.x) {
         bool want = false;
         uint32_t u = 0;
-        if (g < ng && chunks[g]) {  // flat group (ordered groups and empty rows have no chunks)
+        if (g < ng && gtype[g] != kGroupOrdered) {  // flat group (scanned or indexed)
             const uint32_t gs = gr.start[g];
             const uint32_t ge = gr.end[g];
             bool any = false;
@@ -790,13 +867,36 @@ __global__ void del_finish(const RowDesc *desc, const unsigned long long *keys, 
     if (stats) warp_count(&stats[kCntChanged], changed);
 }
 
+// ---------------------------------------------------------------- index upkeep
+// The live entries of an indexed row moved (compaction, relocation): the
+// first positions of its keys are recomputed over the row's first `len`
+// slots at `off` (two passes, reset then minimum).  Block-wide and warp-wide
+// forms; all threads of the block (warp) call.
+__device__ __forceinline__ void idx_reposition_block(const AdjView &view, const PosIndex &ix, uint32_t u,
+                                                     uint64_t off, uint32_t len, Status *st) {
+    for (uint32_t k = threadIdx.x; k < len; k += blockDim.x) idx_pos_reset(ix, u, __ldcg(view.at(off + k)), st);
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < len; k += blockDim.x) idx_pos_set(ix, u, __ldcg(view.at(off + k)), k);
+    __syncthreads();
+}
+
+__device__ __forceinline__ void idx_reposition_warp(const AdjView &view, const PosIndex &ix, uint32_t u,
+                                                    uint64_t off, uint32_t len, Status *st) {
+    const uint32_t lane = lane_id();
+    __syncwarp();
+    for (uint32_t k = lane; k < len; k += 32u) idx_pos_reset(ix, u, __ldcg(view.at(off + k)), st);
+    __syncwarp();
+    for (uint32_t k = lane; k < len; k += 32u) idx_pos_set(ix, u, __ldcg(view.at(off + k)), k);
+    __syncwarp();
+}
+
 // ---------------------------------------------------------------- compaction
 
 // Drop the tombstones of the queued rows in place (order kept).  One block
 // per row; tiles of kTpbMut x 8 slots, block scan, survivors staged in
 // shared memory and stored with coalesced writes.
 __global__ void __launch_bounds__(kTpbMut) compact_rows(AdjView view, RowDesc *desc, const uint32_t *list,
-                                                         const uint32_t *count) {
+                                                         const uint32_t *count, PosIndex ix, Status *st) {
     using BlockScan = cub::BlockScan<uint32_t, kTpbMut>;
     __shared__ typename BlockScan::TempStorage scan_tmp;
     __shared__ uint32_t stage[kTpbMut * kBigItems];
@@ -839,6 +939,7 @@ __global__ void __launch_bounds__(kTpbMut) compact_rows(AdjView view, RowDesc *d
         }
         if (tid == 0) desc[u] = RowDesc{d.off, w, rd_meta(rd_cls(d), 0)};
         __syncthreads();
+        if (idx_row(ix, u)) idx_reposition_block(view, ix, u, d.off, w, st);
     }
 }
 
@@ -929,7 +1030,7 @@ __global__ void alloc_classes(ArenaAlloc *al, Status *st) {
 // for the reverse arena.  A moving row is copied without its tombstones.
 __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long *keys, Groups gr,
                            const unsigned long long *plan, const ArenaAlloc *al, const uint32_t *vals, uint32_t *big,
-                           uint32_t *big_count, unsigned long long *stats, Status *st) {
+                           uint32_t *big_count, unsigned long long *stats, PosIndex ix, Status *st) {
     if (ld_volatile(&st->err) & kErrArena) return;
     const uint32_t lane = lane_id();
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -947,7 +1048,12 @@ __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long
         const RowDesc d = desc[u];
         const uint32_t a = ge - gs;
         if (p == kKeyNone) {
-            for (uint32_t j = lane; j < a; j += 32u) write_slot(view, d.off + d.len + j, vals[key_low(keys[gs + j])]);
+            const bool indexed = idx_row(ix, u);
+            for (uint32_t j = lane; j < a; j += 32u) {
+                const uint32_t v = vals[key_low(keys[gs + j])];
+                write_slot(view, d.off + d.len + j, v);
+                if (indexed) idx_add(ix, u, v, d.len + j, st);
+            }
             if (lane == 0) desc[u] = RowDesc{d.off, d.len + a, d.meta};
         } else {
             if (d.len > kWarpRowMax) {
@@ -966,6 +1072,11 @@ __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long
             }
             for (uint32_t j = lane; j < a; j += 32u) write_slot(view, off + w + j, vals[key_low(keys[gs + j])]);
             if (lane == 0) desc[u] = RowDesc{off, w + a, rd_meta(cls, 0)};
+            if (idx_row(ix, u)) {
+                // survivors moved: reposition them; then count the appended entries
+                idx_reposition_warp(view, ix, u, off, w, st);
+                for (uint32_t j = lane; j < a; j += 32u) idx_add(ix, u, vals[key_low(keys[gs + j])], w + j, st);
+            }
             moved += 1;
         }
         changed += 1;
@@ -979,7 +1090,7 @@ __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long
 __global__ void __launch_bounds__(kTpbMut)
     mutate_add_big(AdjView view, RowDesc *desc, const unsigned long long *keys, Groups gr,
                    const unsigned long long *plan, const ArenaAlloc *al, const uint32_t *vals, const uint32_t *big,
-                   const uint32_t *big_count, unsigned long long *stats, Status *st) {
+                   const uint32_t *big_count, unsigned long long *stats, PosIndex ix, Status *st) {
     using BlockScan = cub::BlockScan<uint32_t, kTpbMut>;
     __shared__ typename BlockScan::TempStorage scan_tmp;
     if (ld_volatile(&st->err) & kErrArena) return;
@@ -1006,6 +1117,11 @@ __global__ void __launch_bounds__(kTpbMut)
         }
         for (uint32_t j = threadIdx.x; j < a; j += kTpbMut) write_slot(view, off + w + j, vals[key_low(keys[gs + j])]);
         __syncthreads();
+        if (idx_row(ix, u)) {
+            idx_reposition_block(view, ix, u, off, w, st);
+            for (uint32_t j = threadIdx.x; j < a; j += kTpbMut) idx_add(ix, u, vals[key_low(keys[gs + j])], w + j, st);
+            __syncthreads();
+        }
         if (threadIdx.x == 0) {
             desc[u] = RowDesc{off, w + a, rd_meta(cls, 0)};
             if (stats) {

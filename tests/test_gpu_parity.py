@@ -272,3 +272,25 @@ def test_autotune_keeps_values_and_parity():
         for i, b in enumerate(case.batches):
             eng.apply_batch(*b)
             assert np.array_equal(eng.values(), trace["batch"][i])
+
+
+INDEX_MODES = {
+    "off": {"CIG_POS_INDEX": "0"},
+    "all_rows": {"CIG_POS_INDEX_CLS": "0"},
+    "all_rows_rebuilt": {"CIG_POS_INDEX_CLS": "0", "CIG_POS_INDEX_HEADROOM": "64"},
+}
+
+
+@pytest.mark.parametrize("mode", list(INDEX_MODES))
+@pytest.mark.parametrize("algo", ["bfs", "sssp", "cc"])
+def test_position_index_modes(algo, mode, monkeypatch):
+    """Deletion positions from the hub-row position index (every row indexed,
+    and with a table small enough that appends force rebuilds) or from the
+    flat scan alone (index off) give the reference's rows and values: parallel
+    edges, repeated requests, compaction and relocation of indexed rows."""
+    for k, v in INDEX_MODES[mode].items():
+        monkeypatch.setenv(k, v)
+    run_case(adversarial_case(), algo, CACHES["resident"])
+    run_case(heavy_delete_case(), algo, CACHES["zerocopy"])
+    run_case_whole_batches(big_row_case(), algo, CACHES["mixed"])
+    run_case_whole_batches(rmat_case(11, 3, 400, 400, seed_offset=17), algo, CACHES["resident"])
