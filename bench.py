@@ -400,7 +400,8 @@ def run_ours(args):
     hbm_peak, peak_kind = load_peaks()
     link_peak = link_peak_gbs(torch, dev)
     stages = {}
-    for name in ("group", "mutate", "mutate_rev", "add", "add_rev", "seed", "inval", "pull", "push", "del_scan"):
+    for name in ("group", "mutate", "mutate_rev", "add", "add_rev", "seed", "inval", "pull", "push", "del_scan",
+                 "index"):
         stages[name] = {"ms_per_batch": prof[name]["ms"] / args.steps, "launches": prof[name]["launches"]}
     kern = {n: stage_roofline(prof[n], hbm_peak, link_peak, "del_scan" if n == "del_scan" else "traversal")
             for n in ("del_scan", "inval", "pull", "push")}

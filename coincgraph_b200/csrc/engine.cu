@@ -269,6 +269,7 @@ struct cig_handle {
     uint32_t *qstamp = nullptr, *aff_stamp = nullptr, *q0 = nullptr, *q1 = nullptr, *list = nullptr;
     uint32_t *small = nullptr;
     unsigned long long *small64 = nullptr;
+    unsigned long long *small64x = nullptr;  // 64 more (per-class slot counts)
     TagState *tags = nullptr;
     Status *status = nullptr;
     Status *h_status = nullptr;
@@ -306,47 +307,69 @@ struct cig_handle {
         uint64_t cap = 0;
         uint64_t rows = 0, entries = 0;  // at the last build
         uint64_t inserted = 0;           // addition requests since (a bound on new keys)
+        uint32_t cls = 0;                // smallest class indexed
         uint64_t builds = 0;
     } ixb[2];  // [0] forward, [1] reverse
     bool use_index = true;
-    uint32_t index_cls = kIdxCls;             // smallest block class indexed
-    uint64_t index_headroom = 1ull << 20;    // table slots beyond twice the entries
+    uint32_t index_cls = kIdxCls;             // smallest block class to index
+    uint64_t index_headroom = 1ull << 20;    // least insert room of a table
+    double index_spare = 1.0;                // insert room per entry
     PosIndex pos_index(bool forward) const {
         const IndexBuf &b = ixb[forward ? 0 : 1];
         return PosIndex{b.keys, b.val, b.cap ? b.cap - 1 : 0, b.rowbit};
     }
 
-    // (Re)build the index of arena A: the rows of class >= index_cls now, a
-    // table of at least twice their slots plus index_headroom (so that appends do not
-    // fill it), if it fits a quarter of the free device memory; otherwise the
-    // arena goes unindexed.  Deleted keys keep their slots until a rebuild,
-    // which mutate_add_arena asks for when the keys inserted since the last
-    // build could take the load factor past one half.  Synchronises.
+    // (Re)build the index of arena A.  A table for e entries has room for
+    // max(index_headroom, index_spare * e) inserts at a load factor of one
+    // half (2 * (e + room) slots, to the next power of two), so that at
+    // steady state a rebuild comes at most once per e inserted keys and its
+    // cost stays a small share of the batches between.  Rows of class >=
+    // index_cls are indexed when their table fits a quarter of the free
+    // device memory; otherwise the threshold rises until it does, and the
+    // arena goes unindexed when no class fits.  Synchronises.
+    uint64_t index_cap(uint64_t e) const {
+        const uint64_t room = std::max<uint64_t>(index_headroom, static_cast<uint64_t>(index_spare * e));
+        uint64_t cap = 1;
+        while (cap < 2 * (e + room)) cap <<= 1;
+        return cap;
+    }
     void build_index(DevArena &A, bool forward) {
         IndexBuf &b = ixb[forward ? 0 : 1];
         if (!use_index) return;
-        CK(cudaMemsetAsync(small64 + 2, 0, sizeof(unsigned long long), stream));
-        launch(idx_count_slots, persistent_grid(), 256, A.desc, n, index_cls, small64 + 2);
-        unsigned long long entries = 0;
-        CK(cudaMemcpyAsync(&entries, small64 + 2, sizeof(entries), cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemsetAsync(small64x, 0, 64 * sizeof(unsigned long long), stream));
+        launch(idx_class_slots, sms * 2, 256, A.desc, n, small64x);
+        unsigned long long hist[64];
+        CK(cudaMemcpyAsync(hist, small64x, sizeof(hist), cudaMemcpyDeviceToHost, stream));
         CK(cudaStreamSynchronize(stream));
-        uint64_t cap = 1;
-        while (cap < 2 * entries + index_headroom) cap <<= 1;
+        size_t fr = 0, tot = 0;
+        CK(cudaMemGetInfo(&fr, &tot));
+        const uint64_t share = (fr + b.cap * (sizeof(unsigned long long) + sizeof(uint2))) / 4;
+        uint64_t entries = 0, cap = 0;
+        uint32_t cls = 64;
+        for (uint32_t c = 63; c + 1 > index_cls; --c) {
+            const uint64_t e = entries + hist[c];
+            const uint64_t cp = index_cap(e);
+            if (cp * (sizeof(unsigned long long) + sizeof(uint2)) > share) break;
+            entries = e;
+            cap = cp;
+            cls = c;
+            if (c == 0) break;
+        }
+        if (entries == 0) {
+            dfree(b.keys);
+            dfree(b.val);
+            dfree(b.rowbit);
+            b = IndexBuf{};
+            return;
+        }
         if (cap > b.cap) {
             dfree(b.keys);
             dfree(b.val);
-            b.cap = 0;
-            size_t fr = 0, tot = 0;
-            CK(cudaMemGetInfo(&fr, &tot));
-            if (entries == 0 || cap * (sizeof(unsigned long long) + sizeof(uint2)) > fr / 4) {
-                dfree(b.rowbit);
-                b = IndexBuf{};
-                return;
-            }
             dmalloc(b.keys, cap);
             dmalloc(b.val, cap);
             b.cap = cap;
         }
+        b.cls = cls;
         const uint32_t words = (n + 31) / 32;
         if (!b.rowbit) dmalloc(b.rowbit, words);
         b.entries = entries;
@@ -355,7 +378,7 @@ struct cig_handle {
         const PosIndex ix = pos_index(forward);
         launch(idx_init, sms * 8, 256, ix);
         CK(cudaMemsetAsync(small + kIdxRows, 0, sizeof(uint32_t), stream));
-        launch(idx_pick_rows, persistent_grid(), 256, A.desc, n, index_cls, b.rowbit, tmp_u32, small + kIdxRows, n,
+        launch(idx_pick_rows, persistent_grid(), 256, A.desc, n, b.cls, b.rowbit, tmp_u32, small + kIdxRows, n,
                status);
         launch(idx_build, sms * 4, 256, A.view(), A.desc, tmp_u32, small + kIdxRows, ix, status);
         check_launch();
@@ -576,6 +599,7 @@ struct cig_handle {
         dmalloc(small, kSmallCount);
         CK(cudaMemset(small, 0, kSmallCount * sizeof(uint32_t)));
         dmalloc(small64, 4);
+        dmalloc(small64x, 64);
         dmalloc(big_rows, kBigRowCap);
         dmalloc(tags, 1);
         CK(cudaMemset(tags, 0, sizeof(TagState)));
@@ -587,6 +611,7 @@ struct cig_handle {
         if (const char *e = std::getenv("CIG_POS_INDEX_CLS")) index_cls = static_cast<uint32_t>(std::atoi(e));
         if (const char *e = std::getenv("CIG_POS_INDEX_HEADROOM"))
             index_headroom = std::max<uint64_t>(64, std::strtoull(e, nullptr, 10));
+        if (const char *e = std::getenv("CIG_POS_INDEX_SPARE")) index_spare = std::max(0.0, std::atof(e));
         if (const char *e = std::getenv("CIG_ASYNC_PER_SM")) async_per_sm = std::max(1, std::atoi(e));
         if (const char *e = std::getenv("CIG_PULL_ON")) tune.pull_on = static_cast<uint32_t>(std::max(0, std::atoi(e)));
         if (const char *e = std::getenv("CIG_PULL_OFF")) tune.pull_off = static_cast<uint32_t>(std::max(1, std::atoi(e)));
@@ -625,6 +650,7 @@ struct cig_handle {
         dfree(list);
         dfree(small);
         dfree(small64);
+        dfree(small64x);
         dfree(big_rows);
         dfree(tags);
         dfree(status);
@@ -1403,7 +1429,11 @@ struct cig_handle {
         if (ixb[forward ? 0 : 1].cap) {
             IndexBuf &b = ixb[forward ? 0 : 1];
             b.inserted += na;
-            if (2 * (b.entries + b.inserted) > b.cap) build_index(A, forward);
+            if (2 * (b.entries + b.inserted) > b.cap) {
+                const int pi = prof_begin(CIG_STAGE_INDEX);
+                build_index(A, forward);
+                prof_end(pi);
+            }
         }
         launch(plan_add, persistent_grid(), 256, A.desc, sorted, grp, plan, A.alloc);
         launch(alloc_classes, 1, 64, A.alloc, status);

@@ -5,7 +5,7 @@
 // position in an unordered row.  For most rows the flat scan (del_scan) is
 // cheap; hub rows are not: on R-MAT s24 they made up most of the ~87 M row
 // entries a 100 k-deletion batch scanned.  Rows whose block class was at
-// least a threshold (default kIdxCls) when the index was last built (`rowbit`)
+// least a threshold when the index was last built (`rowbit`)
 // therefore keep, in one open-addressing hash table per arena, an entry per
 // distinct (u, v): the position of v's first live occurrence in u's row and
 // the number of live occurrences.  Deletions look positions up; appends,
@@ -16,9 +16,9 @@
 // kErrInternal, never a fault).  Values {pos, count} start as {kInf, 0} in
 // every slot, so an insert is a key CAS followed by atomicMin / atomicAdd
 // with no initialisation race.  A slot is never reused after DELETED (so a
-// probe never meets an EMPTY slot before its key); the host rebuilds the
-// table before the keys inserted since the last build can take the load
-// factor past one half.
+// probe never meets an EMPTY slot before its key); the host sizes the table
+// with room for as many inserts as it has entries and rebuilds it before the
+// keys inserted since the last build can take the load factor past one half.
 #pragma once
 
 #include "common.cuh"
@@ -27,7 +27,7 @@ namespace cig {
 
 constexpr unsigned long long kIdxEmpty = ~0ull;
 constexpr unsigned long long kIdxDeleted = ~0ull - 1ull;
-constexpr uint32_t kIdxCls = 12;      // default: rows in blocks of >= 4096 slots are indexed
+constexpr uint32_t kIdxCls = 5;       // default: rows in blocks of >= 32 slots are indexed
 constexpr uint32_t kIdxProbe = 4096;  // probe bound
 
 struct PosIndex {
@@ -109,15 +109,19 @@ __global__ void idx_init(PosIndex ix) {
     }
 }
 
-// Slots of the rows of class >= min_cls (a bound on the keys to index).
-__global__ void idx_count_slots(const RowDesc *desc, uint32_t n, uint32_t min_cls, unsigned long long *total) {
-    unsigned long long t = 0;
+// Slots of the rows of every block class (64 bins), from which the host
+// picks the smallest class threshold whose table fits its memory share.
+__global__ void idx_class_slots(const RowDesc *desc, uint32_t n, unsigned long long *hist) {
+    __shared__ unsigned long long h[64];
+    for (uint32_t i = threadIdx.x; i < 64; i += blockDim.x) h[i] = 0;
+    __syncthreads();
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
         const RowDesc d = desc[v];
-        if (rd_cls(d) >= min_cls) t += d.len;
+        if (d.len) atomicAdd(&h[rd_cls(d)], static_cast<unsigned long long>(d.len));
     }
-    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(kFull, t, o);
-    if (lane_id() == 0 && t) atomicAdd(total, t);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < 64; i += blockDim.x)
+        if (h[i]) atomicAdd(&hist[i], h[i]);
 }
 
 // Rows of class >= min_cls: set their bit and list them.

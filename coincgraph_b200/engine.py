@@ -169,7 +169,7 @@ class QueryStats(ctypes.Structure):
 
 
 STAGES = ["group", "mutate", "seed", "inval", "pull", "push", "pr", "cache", "mutate_rev", "add", "add_rev",
-          "del_scan"]
+          "del_scan", "index"]
 
 
 class StageProfile(ctypes.Structure):

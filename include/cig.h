@@ -305,10 +305,11 @@ enum {
     CIG_STAGE_MUTATE_REV = 8, /* reverse (in-edge) rows */
     CIG_STAGE_ADD = 9,        /* forward rows, addition phase (MUTATE is then the deletion phase) */
     CIG_STAGE_ADD_REV = 10,   /* reverse rows, addition phase */
-    CIG_STAGE_DEL_SCAN = 11,  /* the flat deletion scan kernel alone (inside MUTATE and MUTATE_REV):
-                                 edges = row entries read, edges_cached = of which from HBM,
-                                 hits = deletion keys of the scanned rows */
-    CIG_STAGE_COUNT = 12
+    CIG_STAGE_DEL_SCAN = 11,  /* deletion positions (inside MUTATE and MUTATE_REV): the flat scan
+                                 and the position-index lookups; edges = row entries read,
+                                 edges_cached = of which from HBM, hits = deletion keys */
+    CIG_STAGE_INDEX = 12,     /* position-index rebuilds (inside ADD and ADD_REV) */
+    CIG_STAGE_COUNT = 13
 };
 
 typedef struct {

@@ -277,7 +277,7 @@ def test_autotune_keeps_values_and_parity():
 INDEX_MODES = {
     "off": {"CIG_POS_INDEX": "0"},
     "all_rows": {"CIG_POS_INDEX_CLS": "0"},
-    "all_rows_rebuilt": {"CIG_POS_INDEX_CLS": "0", "CIG_POS_INDEX_HEADROOM": "64"},
+    "all_rows_rebuilt": {"CIG_POS_INDEX_CLS": "0", "CIG_POS_INDEX_HEADROOM": "64", "CIG_POS_INDEX_SPARE": "0"},
 }
 
 
