@@ -605,39 +605,61 @@ __global__ void del_classify(const RowDesc *desc, const unsigned long long *keys
 }
 
 // Indexed rows with distinct requests: the first live position of every key
-// from the index (one warp per group, lanes over its keys); the entry loses
-// one occurrence and, when more remain, moves to the next one (a scan from
-// the deleted position on, rare: parallel edges).
+// from the index; the entry loses one occurrence and, when more remain, moves
+// to the next one (a scan from the deleted position on, rare: parallel
+// edges).  Most groups hold one or two keys, so each lane takes a group of
+// up to kLaneKeys keys alone; larger groups are served by the whole warp.
+constexpr uint32_t kLaneKeys = 4;
+
+__device__ __forceinline__ void del_index_key(const AdjView &view, const RowDesc &d, uint32_t u, uint32_t v,
+                                              uint32_t *fp, const PosIndex &ix, Status *st) {
+    const unsigned long long s = idx_find(ix, (static_cast<unsigned long long>(u) << 32) | v);
+    if (s == ~0ull) return;  // not in the row: a missing delete
+    const uint2 e = ix.val[s];
+    if (e.y == 0u || e.x >= d.len) {
+        if (e.y != 0u) set_error(st, kErrInternal, 0x1d2u);
+        return;
+    }
+    *fp = e.x;
+    if (e.y == 1u) {
+        ix.val[s] = make_uint2(kInf, 0u);
+        ix.keys[s] = kIdxDeleted;
+    } else {
+        uint32_t q = e.x + 1;
+        while (q < d.len && *view.at(d.off + q) != v) ++q;
+        if (q >= d.len) set_error(st, kErrInternal, 0x1d3u);
+        ix.val[s] = make_uint2(q < d.len ? q : kInf, e.y - 1u);
+    }
+}
+
 __global__ void del_index(AdjView view, const RowDesc *desc, const unsigned long long *keys, Groups gr,
                           const uint32_t *list, const uint32_t *count, uint32_t *firstpos, PosIndex ix, Status *st) {
     const uint32_t lane = lane_id();
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t nl = *count;
-    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nl; i += warps) {
-        const uint32_t g = list[i];
-        const uint32_t gs = gr.start[g];
-        const uint32_t nk = gr.end[g] - gs;
-        const uint32_t u = key_src(keys[gs]);
-        const RowDesc d = desc[u];
-        for (uint32_t j = lane; j < nk; j += 32u) {
-            const uint32_t v = key_low(keys[gs + j]);
-            const unsigned long long s = idx_find(ix, (static_cast<unsigned long long>(u) << 32) | v);
-            if (s == ~0ull) continue;  // not in the row: a missing delete
-            const uint2 e = ix.val[s];
-            if (e.y == 0u || e.x >= d.len) {
-                if (e.y != 0u) set_error(st, kErrInternal, 0x1d2u);
-                continue;
-            }
-            firstpos[gs + j] = e.x;
-            if (e.y == 1u) {
-                ix.val[s] = make_uint2(kInf, 0u);
-                ix.keys[s] = kIdxDeleted;
-            } else {
-                uint32_t q = e.x + 1;
-                while (q < d.len && *view.at(d.off + q) != v) ++q;
-                if (q >= d.len) set_error(st, kErrInternal, 0x1d3u);
-                ix.val[s] = make_uint2(q < d.len ? q : kInf, e.y - 1u);
-            }
+    for (uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; base < nl; base += warps * 32u) {
+        const uint32_t i = base + lane;
+        uint32_t gs = 0, nk = 0;
+        if (i < nl) {
+            const uint32_t g = list[i];
+            gs = gr.start[g];
+            nk = gr.end[g] - gs;
+        }
+        if (i < nl && nk <= kLaneKeys) {
+            const uint32_t u = key_src(keys[gs]);
+            const RowDesc d = desc[u];
+            for (uint32_t j = 0; j < nk; ++j) del_index_key(view, d, u, key_low(keys[gs + j]), firstpos + gs + j, ix, st);
+        }
+        uint32_t todo = __ballot_sync(kFull, i < nl && nk > kLaneKeys);
+        while (todo) {
+            const int b = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const uint32_t bs = __shfl_sync(kFull, gs, b);
+            const uint32_t bk = __shfl_sync(kFull, nk, b);
+            const uint32_t u = key_src(keys[bs]);
+            const RowDesc d = desc[u];
+            for (uint32_t j = lane; j < bk; j += 32u)
+                del_index_key(view, d, u, key_low(keys[bs + j]), firstpos + bs + j, ix, st);
         }
     }
 }
@@ -1025,9 +1047,18 @@ __global__ void alloc_classes(ArenaAlloc *al, Status *st) {
     }
 }
 
-// Addition phase, one warp per group (rows above kWarpRowMax that must move
-// go to the block path).  `vals` is add_v for the forward arena and add_u
-// for the reverse arena.  A moving row is copied without its tombstones.
+// Addition phase.  A warp takes 32 groups: each lane serves its own group
+// alone when it is small (at most kLaneAdds appends, and a moving row of at
+// most kLaneRow slots, read into registers with independent loads: rows in
+// host memory cost one round trip, not one per entry), so the common
+// one-request groups run 32 to a warp;
+// the other groups are then served one at a time by the whole warp (rows
+// above kWarpRowMax that must move go to the block path).  `vals` is add_v
+// for the forward arena and add_u for the reverse arena.  A moving row is
+// copied without its tombstones.
+constexpr uint32_t kLaneAdds = 8;
+constexpr uint32_t kLaneRow = 8;
+
 __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long *keys, Groups gr,
                            const unsigned long long *plan, const ArenaAlloc *al, const uint32_t *vals, uint32_t *big,
                            uint32_t *big_count, unsigned long long *stats, PosIndex ix, Status *st) {
@@ -1035,55 +1066,103 @@ __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long
     const uint32_t lane = lane_id();
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t ng = *gr.count;
-    unsigned long long changed = 0, moved = 0;
-    for (uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ng; g += warps) {
-        const unsigned long long p = plan[g];
-        if (p == kKeyNone - 1) {
-            if (lane == 0) set_error(st, kErrInternal, g);
-            continue;
+    uint32_t changed = 0, moved = 0;  // per lane
+    for (uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; base < ng; base += warps * 32u) {
+        const uint32_t g = base + lane;
+        bool coop = false;
+        if (g < ng) {
+            const unsigned long long p = plan[g];
+            const uint32_t gs = gr.start[g];
+            const uint32_t a = gr.end[g] - gs;
+            if (p == kKeyNone - 1) {
+                set_error(st, kErrInternal, g);
+            } else if (a > kLaneAdds) {
+                coop = true;
+            } else {
+                const uint32_t u = key_src(keys[gs]);
+                const RowDesc d = desc[u];
+                const bool indexed = idx_row(ix, u);
+                if (p == kKeyNone) {
+                    for (uint32_t j = 0; j < a; ++j) {
+                        const uint32_t v = vals[key_low(keys[gs + j])];
+                        write_slot(view, d.off + d.len + j, v);
+                        if (indexed) idx_add(ix, u, v, d.len + j, st);
+                    }
+                    desc[u] = RowDesc{d.off, d.len + a, d.meta};
+                    changed += 1;
+                } else if (d.len > kLaneRow) {
+                    coop = true;
+                } else {
+                    const uint32_t cls = static_cast<uint32_t>(p >> 32);
+                    const unsigned long long off = alloc_offset(al, cls, static_cast<uint32_t>(p));
+                    uint32_t row[kLaneRow];
+#pragma unroll
+                    for (uint32_t k = 0; k < kLaneRow; ++k) row[k] = k < d.len ? *view.at(d.off + k) : kTomb;
+                    uint32_t w = 0;
+#pragma unroll
+                    for (uint32_t k = 0; k < kLaneRow; ++k)
+                        if (row[k] != kTomb) write_slot(view, off + w++, row[k]);
+                    for (uint32_t j = 0; j < a; ++j) write_slot(view, off + w + j, vals[key_low(keys[gs + j])]);
+                    desc[u] = RowDesc{off, w + a, rd_meta(cls, 0)};
+                    if (indexed) {
+                        for (uint32_t k = 0; k < w; ++k) idx_pos_reset(ix, u, __ldcg(view.at(off + k)), st);
+                        for (uint32_t k = 0; k < w; ++k) idx_pos_set(ix, u, __ldcg(view.at(off + k)), k);
+                        for (uint32_t j = 0; j < a; ++j) idx_add(ix, u, vals[key_low(keys[gs + j])], w + j, st);
+                    }
+                    moved += 1;
+                    changed += 1;
+                }
+            }
         }
-        const uint32_t gs = gr.start[g];
-        const uint32_t ge = gr.end[g];
-        const uint32_t u = key_src(keys[gs]);
-        const RowDesc d = desc[u];
-        const uint32_t a = ge - gs;
-        if (p == kKeyNone) {
-            const bool indexed = idx_row(ix, u);
-            for (uint32_t j = lane; j < a; j += 32u) {
-                const uint32_t v = vals[key_low(keys[gs + j])];
-                write_slot(view, d.off + d.len + j, v);
-                if (indexed) idx_add(ix, u, v, d.len + j, st);
+        uint32_t todo = __ballot_sync(kFull, coop);
+        while (todo) {
+            const int bl = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const uint32_t gb = base + static_cast<uint32_t>(bl);
+            const unsigned long long p = plan[gb];
+            const uint32_t gs = gr.start[gb];
+            const uint32_t ge = gr.end[gb];
+            const uint32_t u = key_src(keys[gs]);
+            const RowDesc d = desc[u];
+            const uint32_t a = ge - gs;
+            if (p == kKeyNone) {
+                const bool indexed = idx_row(ix, u);
+                for (uint32_t j = lane; j < a; j += 32u) {
+                    const uint32_t v = vals[key_low(keys[gs + j])];
+                    write_slot(view, d.off + d.len + j, v);
+                    if (indexed) idx_add(ix, u, v, d.len + j, st);
+                }
+                if (lane == 0) desc[u] = RowDesc{d.off, d.len + a, d.meta};
+            } else {
+                if (d.len > kWarpRowMax) {
+                    if (lane == 0) big[atomicAdd(big_count, 1u)] = gb;
+                    continue;
+                }
+                const uint32_t cls = static_cast<uint32_t>(p >> 32);
+                const unsigned long long off = alloc_offset(al, cls, static_cast<uint32_t>(p));
+                uint32_t w = 0;
+                for (uint32_t b0 = 0; b0 < d.len; b0 += 32u) {
+                    const uint32_t k = b0 + lane;
+                    const uint32_t x = k < d.len ? *view.at(d.off + k) : kTomb;
+                    const uint32_t km = __ballot_sync(kFull, x != kTomb);
+                    if (x != kTomb) write_slot(view, off + w + __popc(km & lanemask_lt()), x);
+                    w += __popc(km);
+                }
+                for (uint32_t j = lane; j < a; j += 32u) write_slot(view, off + w + j, vals[key_low(keys[gs + j])]);
+                if (lane == 0) desc[u] = RowDesc{off, w + a, rd_meta(cls, 0)};
+                if (idx_row(ix, u)) {
+                    // survivors moved: reposition them; then count the appended entries
+                    idx_reposition_warp(view, ix, u, off, w, st);
+                    for (uint32_t j = lane; j < a; j += 32u) idx_add(ix, u, vals[key_low(keys[gs + j])], w + j, st);
+                }
+                if (lane == 0) moved += 1;
             }
-            if (lane == 0) desc[u] = RowDesc{d.off, d.len + a, d.meta};
-        } else {
-            if (d.len > kWarpRowMax) {
-                if (lane == 0) big[atomicAdd(big_count, 1u)] = g;
-                continue;
-            }
-            const uint32_t cls = static_cast<uint32_t>(p >> 32);
-            const unsigned long long off = alloc_offset(al, cls, static_cast<uint32_t>(p));
-            uint32_t w = 0;
-            for (uint32_t base = 0; base < d.len; base += 32u) {
-                const uint32_t k = base + lane;
-                const uint32_t x = k < d.len ? *view.at(d.off + k) : kTomb;
-                const uint32_t km = __ballot_sync(kFull, x != kTomb);
-                if (x != kTomb) write_slot(view, off + w + __popc(km & lanemask_lt()), x);
-                w += __popc(km);
-            }
-            for (uint32_t j = lane; j < a; j += 32u) write_slot(view, off + w + j, vals[key_low(keys[gs + j])]);
-            if (lane == 0) desc[u] = RowDesc{off, w + a, rd_meta(cls, 0)};
-            if (idx_row(ix, u)) {
-                // survivors moved: reposition them; then count the appended entries
-                idx_reposition_warp(view, ix, u, off, w, st);
-                for (uint32_t j = lane; j < a; j += 32u) idx_add(ix, u, vals[key_low(keys[gs + j])], w + j, st);
-            }
-            moved += 1;
+            if (lane == 0) changed += 1;
         }
-        changed += 1;
     }
-    if (lane == 0 && stats) {
-        if (changed) atomicAdd(&stats[kCntChanged], changed);
-        if (moved) atomicAdd(&stats[kCntRelocated], moved);
+    if (stats) {
+        warp_count(&stats[kCntChanged], changed);
+        warp_count(&stats[kCntRelocated], moved);
     }
 }
 

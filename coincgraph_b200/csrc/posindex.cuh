@@ -139,11 +139,26 @@ __global__ void idx_pick_rows(const RowDesc *desc, uint32_t n, uint32_t min_cls,
 // Entries of the listed rows; one block per row.
 __global__ void idx_build(AdjView view, const RowDesc *desc, const uint32_t *list, const uint32_t *count,
                           PosIndex ix, Status *st) {
+    // Rows of at least kIdxBlockRow entries: a block each; shorter rows (most
+    // of them) a warp each, so that lanes are not left idle on short rows.
+    constexpr uint32_t kIdxBlockRow = 512;
     const uint32_t nr = *count;
     for (uint32_t r = blockIdx.x; r < nr; r += gridDim.x) {
         const uint32_t u = list[r];
         const RowDesc d = desc[u];
+        if (d.len < kIdxBlockRow) continue;
         for (uint32_t k = threadIdx.x; k < d.len; k += blockDim.x) {
+            const uint32_t v = *view.at(d.off + k);
+            if (v != kTomb) idx_add(ix, u, v, k, st);
+        }
+    }
+    const uint32_t lane = lane_id();
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nr; r += warps) {
+        const uint32_t u = list[r];
+        const RowDesc d = desc[u];
+        if (d.len >= kIdxBlockRow) continue;
+        for (uint32_t k = lane; k < d.len; k += 32u) {
             const uint32_t v = *view.at(d.off + k);
             if (v != kTomb) idx_add(ix, u, v, k, st);
         }
