@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <chrono>
 #include <condition_variable>
+#include <functional>
 #include <cstring>
 #include <deque>
 #include <memory>
@@ -618,6 +619,7 @@ struct cig_handle {
     }
 
     void destroy() {
+        stager_stop();
         cudaSetDevice(device);
         if (stream) cudaStreamSynchronize(stream);
         for (auto &e : ev)
@@ -1493,26 +1495,91 @@ struct cig_handle {
     }
 
     // Copy host update arrays into the device batch buffers (pinned staging).
-    void stage_pairs(const uint32_t *hu, const uint32_t *hv, uint64_t count, uint32_t *du_, uint32_t *dv_,
-                     uint32_t *stage_base) {
-        if (!count) return;
-        if (!hu || !hv) throw CigError(CIG_ERR_ARG, "null update array");
-        // Large batches: four threads fill the pinned staging buffer.
-        auto copy = [&](uint64_t b, uint64_t e) {
-            std::memcpy(stage_base + b, hu + b, (e - b) * sizeof(uint32_t));
-            std::memcpy(stage_base + bcap + b, hv + b, (e - b) * sizeof(uint32_t));
-        };
-        if (count >= (1u << 16)) {
-            std::thread th[3];
-            const uint64_t q = (count + 3) / 4;
-            for (int t = 0; t < 3; ++t) th[t] = std::thread(copy, t * q, std::min<uint64_t>(count, (t + 1) * q));
-            copy(std::min<uint64_t>(count, 3 * q), count);
-            for (auto &t : th) t.join();
-        } else {
-            copy(0, count);
+    // Host update arrays go through the pinned staging buffer.  Reading the
+    // caller's arrays (cold in host DRAM) is what costs: one thread moves
+    // ~6 GB/s, so the calling thread and kStageWorkers persistent workers
+    // each copy one part of every array.  The workers spin for kStageSpin
+    // after a job before they sleep on a condition variable, so in a stream
+    // of batches a call finds them awake (a wake-up from sleep costs about
+    // what the split saves).  Then the host-to-device copies are queued on
+    // the engine stream.  The previous call's copies have completed (every
+    // call ends with a synchronisation), so the buffer is free.
+    static constexpr int kStageWorkers = 3;
+    static constexpr auto kStageSpin = std::chrono::milliseconds(3);
+    struct Stager {
+        std::vector<std::thread> threads;
+        std::mutex m;
+        std::condition_variable go;
+        std::atomic<uint64_t> gen{0};
+        std::atomic<int> pending{0};
+        std::atomic<bool> stop{false};
+        std::function<void(int)> job;
+    } stager;
+
+    void stager_run(const std::function<void(int)> &job) {
+        Stager &S = stager;
+        if (S.threads.empty())
+            for (int w = 0; w < kStageWorkers; ++w)
+                S.threads.emplace_back([&S, w] {
+                    uint64_t seen = 0;
+                    for (;;) {
+                        const auto t0 = std::chrono::steady_clock::now();
+                        while (S.gen.load(std::memory_order_acquire) == seen && !S.stop.load(std::memory_order_relaxed) &&
+                               std::chrono::steady_clock::now() - t0 < kStageSpin)
+                            std::this_thread::yield();
+                        if (S.gen.load(std::memory_order_acquire) == seen) {
+                            std::unique_lock<std::mutex> lk(S.m);
+                            S.go.wait(lk, [&] { return S.stop.load() || S.gen.load() != seen; });
+                        }
+                        if (S.stop.load()) return;
+                        seen = S.gen.load(std::memory_order_acquire);
+                        S.job(w + 1);  // unchanged until every worker reported
+                        S.pending.fetch_sub(1, std::memory_order_release);
+                    }
+                });
+        S.job = job;
+        S.pending.store(kStageWorkers, std::memory_order_relaxed);
+        {
+            std::lock_guard<std::mutex> lk(S.m);
+            S.gen.fetch_add(1, std::memory_order_release);
         }
-        CK(cudaMemcpyAsync(du_, stage_base, count * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
-        CK(cudaMemcpyAsync(dv_, stage_base + bcap, count * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        S.go.notify_all();
+        job(0);
+        while (S.pending.load(std::memory_order_acquire) != 0) std::this_thread::yield();
+    }
+
+    void stager_stop() {
+        {
+            std::lock_guard<std::mutex> lk(stager.m);
+            stager.stop.store(true);
+        }
+        stager.go.notify_all();
+        for (auto &t : stager.threads) t.join();
+        stager.threads.clear();
+    }
+
+    void stage_batch(const uint32_t *hdu, const uint32_t *hdv, uint64_t nd, const uint32_t *hau, const uint32_t *hav,
+                     uint64_t na) {
+        if ((nd && (!hdu || !hdv)) || (na && (!hau || !hav))) throw CigError(CIG_ERR_ARG, "null update array");
+        const uint32_t *src[4] = {hdu, hdv, hau, hav};
+        const uint64_t cnt[4] = {nd, nd, na, na};
+        uint32_t *dst[4] = {stage, stage + bcap, stage + 2 * bcap, stage + 3 * bcap};
+        auto copy = [&](int part, int parts) {
+            for (int a = 0; a < 4; ++a) {
+                const uint64_t q = (cnt[a] + parts - 1) / parts;
+                const uint64_t b = std::min<uint64_t>(cnt[a], static_cast<uint64_t>(part) * q);
+                const uint64_t e = std::min<uint64_t>(cnt[a], b + q);
+                if (e > b) std::memcpy(dst[a] + b, src[a] + b, (e - b) * sizeof(uint32_t));
+            }
+        };
+        if (nd + na >= (1u << 16))
+            stager_run([&](int part) { copy(part, kStageWorkers + 1); });
+        else
+            copy(0, 1);
+        uint32_t *dev[4] = {du, dv, au, av};
+        for (int a = 0; a < 4; ++a)
+            if (cnt[a])
+                CK(cudaMemcpyAsync(dev[a], dst[a], cnt[a] * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
     }
 
     void require_ready() {
@@ -1526,7 +1593,7 @@ struct cig_handle {
         ensure_batch(nd);
         reset_counters();
         CK(cudaEventRecord(ev[0], stream));
-        stage_pairs(hu, hv, nd, du, dv, stage);
+        stage_batch(hu, hv, nd, nullptr, nullptr, 0);
         dispatch([&](auto tag) { delete_phase_dev<decltype(tag)::value>(du, dv, nd); });
         CK(cudaEventRecord(ev[1], stream));
         finish();
@@ -1539,7 +1606,7 @@ struct cig_handle {
         ensure_batch(na);
         reset_counters();
         CK(cudaEventRecord(ev[1], stream));
-        stage_pairs(hu, hv, na, au, av, stage + 2 * bcap);
+        stage_batch(nullptr, nullptr, 0, hu, hv, na);
         dispatch([&](auto tag) { insert_phase_dev<decltype(tag)::value>(au, av, na); });
         CK(cudaEventRecord(ev[2], stream));
         run_cache_service();
@@ -1584,8 +1651,7 @@ struct cig_handle {
         ensure_batch(std::max(nd, na));
         reset_counters();
         CK(cudaEventRecord(ev[0], stream));
-        stage_pairs(hdu, hdv, nd, du, dv, stage);
-        stage_pairs(hau, hav, na, au, av, stage + 2 * bcap);
+        stage_batch(hdu, hdv, nd, hau, hav, na);
         apply_batch(du, dv, nd, au, av, na, s, mutation_after);
     }
 
