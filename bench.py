@@ -57,10 +57,12 @@ def parse_args():
     p.add_argument("--ref-budget-s", type=float, default=150.0,
                    help="reference arm: stop timing after this much CPU time")
     p.add_argument("--workload", default="stream",
-                   choices=["stream", "msbfs", "mssssp", "uneven", "served", "pr"],
+                   choices=["stream", "road", "msbfs", "mssssp", "uneven", "served", "pr"],
                    help="stream: the update-stream benchmark (default); msbfs/mssssp: 64-source queries "
                         "on a symmetric R-MAT graph, batched bitmask waves vs the per-source form; uneven: "
-                        "batches of log-uniform sizes, batched form (one sync) vs one call per batch")
+                        "batches of log-uniform sizes, batched form (one sync) vs one call per batch; road: the "
+                        "update stream on a high-diameter grid graph (--side) with local insertions")
+    p.add_argument("--side", type=int, default=2048, help="road: grid side (side^2 vertices)")
     p.add_argument("--requests", type=int, default=400, help="served: requests in the stream")
     p.add_argument("--update-frac", type=float, default=0.1, help="served: share of update requests")
     p.add_argument("--rate", type=float, default=0.0, help="served: Poisson arrival rate, requests/s (0: all at once)")
@@ -105,6 +107,13 @@ def make_workload(args, nbatches):
     from coincgraph_b200 import gen
 
     t0 = time.perf_counter()
+    if args.workload == "road":
+        g = gen.grid(args.side)
+        t1 = time.perf_counter()
+        ups = gen.local_updates(g, args.side, [args.batch] * nbatches, [args.batch] * nbatches,
+                                seed=gen.UPDATE_SEED_BASE + 7)
+        t2 = time.perf_counter()
+        return g, ups, {"gen_graph_s": round(t1 - t0, 2), "gen_updates_s": round(t2 - t1, 2)}
     g, h = gen.rmat(args.scale, args.edge_factor, keep_handle=True)
     t1 = time.perf_counter()
     ups = gen.updates(h, [args.batch] * nbatches, [args.batch] * nbatches, seed=gen.UPDATE_SEED_BASE + 2)
@@ -310,7 +319,9 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": len(times), "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": WORKLOAD if args.scale == 24 else f"{WORKLOAD} (scale {args.scale})",
+        "config": {"workload": (f"incremental {args.algo.upper()}, road-like grid {args.side}x{args.side}, "
+                                f"{args.batch} del + {args.batch} ins per batch") if args.workload == "road" else
+                   WORKLOAD if args.scale == 24 else f"{WORKLOAD} (scale {args.scale})",
                    "scale": args.scale, "batch": args.batch, "algo": args.algo, "setup": setup},
         "p50_ms": statistics.median(times) * 1e3, "p99_ms": float(np.percentile(np.array(times) * 1e3, 99)),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "reference" if have_ref else "port",
@@ -446,9 +457,11 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": WORKLOAD if args.scale == 24 and args.batch == 100_000 else
-                       f"incremental {args.algo.upper()}, RMAT s{args.scale} ef{args.edge_factor}, cache "
-                       f"{args.cache} GiB, {args.batch} del + {args.batch} ins per batch",
+            "config": {"workload": WORKLOAD if args.workload == "stream" and args.scale == 24 and args.batch == 100_000
+                       else f"incremental {args.algo.upper()}, "
+                       + (f"road-like grid {args.side}x{args.side}" if args.workload == "road" else
+                          f"RMAT s{args.scale} ef{args.edge_factor}")
+                       + f", cache {args.cache} GiB, {args.batch} del + {args.batch} ins per batch",
                        "algo": args.algo, "vertices": g.n, "edges": g.m, "cache_gib": args.cache,
                        "segments_resident": info["segments_resident"], "segments_total": info["segments_total"],
                        "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
@@ -777,7 +790,7 @@ def main():
             return
         run_uneven(args)
         return
-    if args.workload != "stream":
+    if args.workload not in ("stream", "road"):
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "query workloads have no reference CPU arm"}))
             return

@@ -189,6 +189,7 @@ enum SmallIdx : int {
     kOrderedCount = 17,
     kIndexedCount = 20,  // deletion groups answered by the position index
     kIdxRows = 21,       // rows of an arena being indexed (load time)
+    kInvalDone = 22,     // vertices expanded by the invalidation closure's local sweeps
     kGaF = 18,  // addition-phase group counts of a presorted batch
     kGaR = 19,
     kSmallCount = 24
@@ -608,6 +609,7 @@ struct cig_handle {
         if (const char *e = std::getenv("CIG_COOP_BLOCKS_PER_SM")) tune.per_sm = std::max(1, std::atoi(e));
         if (const char *e = std::getenv("CIG_SPLIT_DEG")) tune.split = std::max(32, std::atoi(e));
         if (const char *e = std::getenv("CIG_ASYNC_PUSH")) async_push = std::atoi(e) != 0;
+        if (const char *e = std::getenv("CIG_LOCAL_SWEEPS")) local_sweeps = static_cast<uint32_t>(std::max(0, std::atoi(e)));
         if (const char *e = std::getenv("CIG_POS_INDEX")) use_index = std::atoi(e) != 0;
         if (const char *e = std::getenv("CIG_POS_INDEX_CLS")) index_cls = static_cast<uint32_t>(std::atoi(e));
         if (const char *e = std::getenv("CIG_POS_INDEX_HEADROOM"))
@@ -669,6 +671,7 @@ struct cig_handle {
         dfree(pr_queued);
         free_batch();
         dfree(tmp_u32);
+        dfree(inval_done);
         dfree(chunk_map);
         for (auto &b : ixb) {
             dfree(b.keys);
@@ -912,6 +915,7 @@ struct cig_handle {
         dmalloc(q0, n + 1);
         dmalloc(q1, n + 1);
         dmalloc(tmp_u32, n);
+        if (local_sweeps && opt.algo != CIG_PR) dmalloc(inval_done, n + 1);
         build_index(fwd, true);
         if (opt.algo != CIG_PR) build_index(rev, false);
         if (opt.algo == CIG_PR) {
@@ -1056,12 +1060,14 @@ struct cig_handle {
             launch(push_async<A>, sms * async_per_sm, kTpb, fwd.view(), state, qstamp, tags, ring, seg_hot, status);
             launch(advance_tag, 1, 1, tags, 2u);
         } else {
-            launch_coop(push_closure<A>, kTpb, fwd.view(), state, qstamp, tags, frontier(), big_list(), n + 2, seg_hot,
-                        status);
+            launch_coop(push_closure<A>, kTpb, fwd.view(), state, qstamp, tags, frontier(), big_list(), n + 2,
+                        local_sweeps, seg_hot, status);
         }
         prof_end(p);
     }
     bool async_push = false;  // measured equal to the level-synchronous closure on RMAT (CIG_ASYNC_PUSH=1)
+    uint32_t local_sweeps = 8;  // block-local hops per closure round (CIG_LOCAL_SWEEPS; 0 = off)
+    uint32_t *inval_done = nullptr;  // n + 1: vertices the invalidation sweeps expanded
     int async_per_sm = 2;  // worker blocks per SM of the asynchronous closure
     unsigned long long *ring_slot = nullptr;  // ring_cap slots, all zero between closures
     uint32_t ring_cap = 0;
@@ -1465,8 +1471,10 @@ struct cig_handle {
         mutate_delete_arena(fwd, d_du, d_dv, nd, true, true);
         mutate_delete_arena(rev, d_du, d_dv, nd, false, false);
         p = prof_begin(CIG_STAGE_INVAL);
+        if (local_sweeps) CK(cudaMemsetAsync(small + kInvalDone, 0, sizeof(uint32_t), stream));
         launch_coop(inval_closure<A>, kTpb, fwd.view(), state, aff_stamp, epoch, list, small + kAff, n + 1,
-                    big_list(), n + 2, small + kAffTotal, seg_hot, status);
+                    big_list(), n + 2, local_sweeps, inval_done, small + kInvalDone, small + kAffTotal, seg_hot,
+                    status);
         prof_end(p);
         p = prof_begin(CIG_STAGE_PULL);
         launch(reset_affected<A>, persistent_grid(), 256, list, small + kAffTotal, state);

@@ -142,14 +142,74 @@ struct BigList {
     uint32_t split;  // deferral threshold (row entries), tuned per handle
 };
 
+// Block-local sweeps.  After a block has relaxed its share of a round's
+// frontier, the vertices it improved (and that are not already queued for
+// the next round) go to a queue in its shared memory, and the block expands
+// them itself for up to `max_sweeps` more hops, synchronising with
+// __syncthreads only; what is left (or does not fit) goes to the next
+// round's frontier as usual.  On high-diameter graphs, whose rounds carry
+// small frontiers and cost a chain of dependent memory accesses plus a grid
+// barrier each, this covers several hops per grid round.  A vertex may then
+// be expanded by two blocks in one round (a redundant relaxation); the
+// label-correcting fixpoint, values and smallest-id parents, is unchanged.
+constexpr uint32_t kLocalCap = 1024;
+constexpr uint32_t kSweepItems = 4;  // invalidation sweeps: rounds of at most this many items per block
+
+template <int A>
+struct LocalPushOp {
+    unsigned long long *state;
+    uint32_t *qstamp;
+    uint32_t tag;       // membership of the next round's frontier
+    uint32_t *q_out;    // next round's frontier (overflow)
+    uint32_t *q_count;
+    uint32_t q_cap;
+    uint32_t *lq;       // shared-memory queue of this sweep's output
+    uint32_t *lq_n;
+    Status *st;
+
+    __device__ __forceinline__ bool edge(bool valid, uint32_t x, uint32_t dx, uint32_t y) const {
+        bool want = false, improved = false;
+        if (valid) {
+            const uint32_t nd = dx + edge_weight<A>(x, y);
+            const unsigned long long cand = pack(nd, x);
+            if (cand < __ldcg(state + y)) {
+                const unsigned long long old = atomicMin(state + y, cand);
+                improved = nd < val_of(old);
+                want = improved && __ldcg(qstamp + y) != tag;
+            }
+        }
+        const uint32_t mask = __ballot_sync(kFull, want);
+        bool spill = false;
+        if (mask) {
+            const uint32_t lane = lane_id();
+            const uint32_t leader = __ffs(mask) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(lq_n, __popc(mask));
+            base = __shfl_sync(kFull, base, leader);
+            if (want) {
+                const uint32_t pos = base + __popc(mask & lanemask_lt());
+                if (pos < kLocalCap)
+                    lq[pos] = y;
+                else
+                    spill = atomicExch(qstamp + y, tag) != tag;
+            }
+        }
+        warp_enqueue(spill, y, q_out, q_count, q_cap, st);
+        return improved;
+    }
+};
+
 template <int A>
 __global__ void __launch_bounds__(kTpb) push_closure(AdjView fwd, unsigned long long *state, uint32_t *qstamp,
                                                      TagState *tags, Frontier fr, BigList big, uint32_t max_rounds,
-                                                     uint32_t *seg_hot, Status *st) {
+                                                     uint32_t max_sweeps, uint32_t *seg_hot, Status *st) {
     __shared__ ExpandSmem<kTpb> sm;
+    __shared__ uint32_t lq[2][kLocalCap];
+    __shared__ uint32_t lq_n[2];
     ExpandCounters cnt;
     // next_tag itself belongs to the seeds queued before this launch.
     const uint32_t tag0 = tags->next_tag + 1;
+    const uint32_t sweeps = max_sweeps;
     uint32_t r = 0;
     for (;; ++r) {
         const uint32_t n_in = ld_volatile(fr.cnt + (r % 3));
@@ -163,8 +223,14 @@ __global__ void __launch_bounds__(kTpb) push_closure(AdjView fwd, unsigned long 
             big.cnt[(r + 2) % 3] = 0;
         }
         const uint32_t *in = (r & 1) ? fr.q1 : fr.q0;
-        PushOp<A> op{state, qstamp, tag0 + r, (r & 1) ? fr.q0 : fr.q1, fr.cnt + ((r + 1) % 3), fr.cap, st};
+        uint32_t *out = (r & 1) ? fr.q0 : fr.q1;
+        uint32_t *out_cnt = fr.cnt + ((r + 1) % 3);
+        PushOp<A> op{state, qstamp, tag0 + r, out, out_cnt, fr.cap, st};
         const Defer df{big.rows, big.cnt + (r % 3), big.cap, big.split};
+        if (sweeps) {
+            if (threadIdx.x == 0) lq_n[0] = 0;
+            __syncthreads();
+        }
         // Item i goes to block i mod gridDim.x, so small frontiers still
         // spread over the whole grid.
         for (uint32_t base = 0; base < n_in; base += gridDim.x * kTpb) {
@@ -181,7 +247,49 @@ __global__ void __launch_bounds__(kTpb) push_closure(AdjView fwd, unsigned long 
                 has = dx != kInf && deg > 0;
                 if (has && seg_hot) atomicAdd(seg_hot + (off >> kSegShift), deg);
             }
-            expand_rows<kTpb>(fwd, has, x, dx, off, deg, op, sm, cnt, df);
+            if (sweeps)
+                expand_rows<kTpb>(fwd, has, x, dx, off, deg,
+                                  LocalPushOp<A>{state, qstamp, tag0 + r, out, out_cnt, fr.cap, lq[0], &lq_n[0], st},
+                                  sm, cnt, df);
+            else
+                expand_rows<kTpb>(fwd, has, x, dx, off, deg, op, sm, cnt, df);
+        }
+        if (sweeps) {
+            uint32_t cur = 0;
+            for (uint32_t sw = 0; sw < sweeps; ++sw) {
+                __syncthreads();
+                const uint32_t nl = min(lq_n[cur], kLocalCap);
+                if (nl == 0) break;
+                if (threadIdx.x == 0) lq_n[cur ^ 1u] = 0;
+                __syncthreads();
+                const LocalPushOp<A> lop{state, qstamp, tag0 + r, out, out_cnt, fr.cap, lq[cur ^ 1u], &lq_n[cur ^ 1u], st};
+                for (uint32_t base = 0; base < nl; base += kTpb) {
+                    const uint32_t i = base + threadIdx.x;
+                    bool has = i < nl;
+                    uint32_t x = 0, dx = 0, deg = 0;
+                    uint64_t off = 0;
+                    if (has) {
+                        x = lq[cur][i];
+                        dx = val_of(__ldcg(state + x));
+                        const RowDesc d = fwd.desc[x];
+                        deg = d.len;
+                        off = d.off;
+                        has = dx != kInf && deg > 0;
+                        if (has && seg_hot) atomicAdd(seg_hot + (off >> kSegShift), deg);
+                    }
+                    expand_rows<kTpb>(fwd, has, x, dx, off, deg, lop, sm, cnt, df);
+                }
+                cur ^= 1u;
+            }
+            // What the last sweep queued joins the next round's frontier.
+            __syncthreads();
+            const uint32_t nl = min(lq_n[cur], kLocalCap);
+            for (uint32_t b0 = 0; b0 < nl; b0 += kTpb) {
+                const uint32_t i = b0 + threadIdx.x;
+                const uint32_t y = i < nl ? lq[cur][i] : 0u;
+                const bool want = i < nl && atomicExch(qstamp + y, tag0 + r) != tag0 + r;
+                warp_enqueue(want, y, out, out_cnt, fr.cap, st);
+            }
         }
         if (!grid_barrier(st)) break;
         const uint32_t nbig = min(ld_volatile(big.cnt + (r % 3)), big.cap);
@@ -388,12 +496,66 @@ __global__ void __launch_bounds__(kTpb, 4) push_async(AdjView fwd, unsigned long
 // Persistent invalidation closure over the affected list.  Round r processes
 // list[lo, hi) and appends at list[hi + ...] counted by cnt[(r+1)%3].
 // Replaces RunSyncPushDDB_del rounds (framework.cuh:2830-2853).
+// Local sweeps of the invalidation closure: a vertex a block claims goes to
+// the block's shared-memory queue and is expanded by the block at once, for
+// up to `max_sweeps` hops (then appended to `done`); what is left after the
+// last sweep, or does not fit, goes to the next round's list as usual.
+// Every claimed vertex is expanded once and ends in exactly one of the two
+// lists; `done` is appended to the list when the closure ends, so the
+// affected list is the same set.
+template <int A>
+struct LocalInvalOp {
+    unsigned long long *state;
+    uint32_t *aff_stamp;
+    uint32_t epoch;
+    uint32_t *list;
+    uint32_t *count;
+    uint32_t cap;
+    uint32_t *lq;
+    uint32_t *lq_n;
+    Status *st;
+
+    __device__ __forceinline__ bool edge(bool valid, uint32_t x, uint32_t px, uint32_t z) const {
+        bool want = false;
+        if (valid) {
+            const unsigned long long sz = __ldcg(state + z);
+            bool dep;
+            if (A == kCc)
+                dep = z != x && val_of(sz) == px && px < z;
+            else
+                dep = par_of(sz) == x;
+            if (dep && __ldcg(aff_stamp + z) != epoch) want = atomicExch(aff_stamp + z, epoch) != epoch;
+        }
+        const uint32_t mask = __ballot_sync(kFull, want);
+        bool spill = false;
+        if (mask) {
+            const uint32_t lane = lane_id();
+            const uint32_t leader = __ffs(mask) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(lq_n, __popc(mask));
+            base = __shfl_sync(kFull, base, leader);
+            const uint32_t pos = base + __popc(mask & lanemask_lt());
+            if (want) {
+                if (pos < kLocalCap)
+                    lq[pos] = z;
+                else
+                    spill = true;
+            }
+        }
+        warp_enqueue(spill, z, list, count, cap, st);
+        return want;
+    }
+};
+
 template <int A>
 __global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long long *state, uint32_t *aff_stamp,
                                                       uint32_t epoch, uint32_t *list, uint32_t *cnt3,
                                                       uint32_t cap, BigList big, uint32_t max_rounds,
+                                                      uint32_t max_sweeps, uint32_t *done, uint32_t *done_cnt,
                                                       uint32_t *aff_total, uint32_t *seg_hot, Status *st) {
     __shared__ ExpandSmem<kTpb> sm;
+    __shared__ uint32_t lq[2][kLocalCap];
+    __shared__ uint32_t lq_n[2];
     ExpandCounters c;
     uint32_t lo = 0, hi = ld_volatile(cnt3 + 0);
     uint32_t r = 0;
@@ -410,6 +572,14 @@ __global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long
         InvalOp<A> op{state, aff_stamp, epoch, list + hi, cnt3 + ((r + 1) % 3), cap > hi ? cap - hi : 0u, st};
         const Defer df{big.rows, big.cnt + (r % 3), big.cap, big.split};
         const uint32_t n_in = hi - lo;
+        // Sweeps only for small frontiers (a few items per block): on R-MAT
+        // the large invalidation rounds already fill the grid, and sweeps
+        // left their work to the blocks that found it (2x slower there).
+        const uint32_t sweeps = n_in <= kSweepItems * gridDim.x ? max_sweeps : 0u;
+        if (sweeps) {
+            if (threadIdx.x == 0) lq_n[0] = 0;
+            __syncthreads();
+        }
         for (uint32_t base = 0; base < n_in; base += gridDim.x * kTpb) {
             const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
             bool has = i < n_in;
@@ -424,7 +594,50 @@ __global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long
                 has = deg > 0;
                 if (has && seg_hot) atomicAdd(seg_hot + (off >> kSegShift), deg);
             }
-            expand_rows<kTpb>(fwd, has, x, px, off, deg, op, sm, c, df);
+            if (sweeps)
+                expand_rows<kTpb>(fwd, has, x, px, off, deg,
+                                  LocalInvalOp<A>{state, aff_stamp, epoch, op.list, op.count, op.cap, lq[0], &lq_n[0],
+                                                  st},
+                                  sm, c, df);
+            else
+                expand_rows<kTpb>(fwd, has, x, px, off, deg, op, sm, c, df);
+        }
+        if (sweeps) {
+            uint32_t cur = 0;
+            for (uint32_t sw = 0; sw < sweeps; ++sw) {
+                __syncthreads();
+                const uint32_t nl = min(lq_n[cur], kLocalCap);
+                if (nl == 0) break;
+                if (threadIdx.x == 0) lq_n[cur ^ 1u] = 0;
+                __syncthreads();
+                const LocalInvalOp<A> lop{state, aff_stamp, epoch, op.list, op.count, op.cap, lq[cur ^ 1u],
+                                          &lq_n[cur ^ 1u], st};
+                for (uint32_t base = 0; base < nl; base += kTpb) {
+                    const uint32_t i = base + threadIdx.x;
+                    bool has = i < nl;
+                    uint32_t x = 0, px = 0, deg = 0;
+                    uint64_t off = 0;
+                    if (has) x = lq[cur][i];
+                    warp_enqueue(has, x, done, done_cnt, cap, st);
+                    if (has) {
+                        px = (A == kCc) ? val_of(__ldcg(state + x)) : x;
+                        const RowDesc d = fwd.desc[x];
+                        deg = d.len;
+                        off = d.off;
+                        has = deg > 0;
+                        if (has && seg_hot) atomicAdd(seg_hot + (off >> kSegShift), deg);
+                    }
+                    expand_rows<kTpb>(fwd, has, x, px, off, deg, lop, sm, c, df);
+                }
+                cur ^= 1u;
+            }
+            // What the last sweep claimed is expanded by the next round.
+            __syncthreads();
+            const uint32_t nl = min(lq_n[cur], kLocalCap);
+            for (uint32_t b0 = 0; b0 < nl; b0 += kTpb) {
+                const uint32_t i = b0 + threadIdx.x;
+                warp_enqueue(i < nl, i < nl ? lq[cur][i] : 0u, op.list, op.count, op.cap, st);
+            }
         }
         if (!grid_barrier(st)) break;
         const uint32_t nbig = min(ld_volatile(big.cnt + (r % 3)), big.cap);
@@ -434,6 +647,15 @@ __global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long
         }
         lo = hi;
         hi = hi + ld_volatile(cnt3 + ((r + 1) % 3));
+    }
+    if (max_sweeps) {
+        // The vertices expanded by local sweeps complete the affected list.
+        // Every block left the loop after the same barrier, so `done` is final.
+        const uint32_t nd = ld_volatile(done_cnt);
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nd && hi + i < cap; i += gridDim.x * blockDim.x)
+            list[hi + i] = __ldcg(done + i);
+        if (hi + nd > cap && blockIdx.x == 0 && threadIdx.x == 0) set_error(st, kErrQueue, hi + nd);
+        hi += min(nd, cap - min(hi, cap));
     }
     flush_counters(st, c, kCntInval);
     if (blockIdx.x == 0 && threadIdx.x == 0) {

@@ -134,6 +134,57 @@ def updates(graph_handle, del_sizes, add_sizes, seed: int, symmetric: bool = Fal
     return UpdateStream(du[:nd], dv[:nd], au[:na], av[:na], del_off, add_off)
 
 
+def grid(side: int, seed: int | None = None) -> Graph:
+    """Road-like graph: a side x side grid, each vertex joined both ways to
+    its 4 neighbours (rows in east, west, south, north order), vertex
+    i * side + j at row i, column j.  High diameter (2 * side hops) and
+    degree <= 4, unlike R-MAT."""
+    n = side * side
+    i, j = np.divmod(np.arange(n, dtype=np.int64), side)
+    cand = np.stack([np.where(j + 1 < side, i * side + j + 1, -1), np.where(j > 0, i * side + j - 1, -1),
+                     np.where(i + 1 < side, (i + 1) * side + j, -1), np.where(i > 0, (i - 1) * side + j, -1)], axis=1)
+    deg = (cand >= 0).sum(axis=1)
+    xadj = np.zeros(n + 1, dtype=np.uint64)
+    xadj[1:] = np.cumsum(deg)
+    adj = cand[cand >= 0].astype(np.uint32)
+    return Graph(n, xadj, adj)
+
+
+def local_updates(g: Graph, side: int, del_sizes, add_sizes, seed: int, reach: int = 3) -> UpdateStream:
+    """Update batches for a grid: deletions of distinct existing edges in a
+    seeded random order (each edge deleted at most once), insertions of new
+    pairs (u, v) with v within `reach` rows and columns of u (road-like
+    shortcuts), never an existing or already inserted pair."""
+    rng = np.random.default_rng(seed)
+    src = np.repeat(np.arange(g.n, dtype=np.uint64), np.diff(g.xadj).astype(np.int64))
+    order = rng.permutation(g.m)
+    nd, na = int(np.sum(del_sizes)), int(np.sum(add_sizes))
+    pick = order[:nd]
+    du, dv = src[pick].astype(np.uint32), g.adj[pick]
+    existing = set((src.astype(np.uint64) << np.uint64(32) | g.adj.astype(np.uint64)).tolist())
+    au, av = np.empty(na, dtype=np.uint32), np.empty(na, dtype=np.uint32)
+    k = 0
+    while k < na:
+        u = rng.integers(0, g.n, size=2 * (na - k) + 16)
+        di = rng.integers(-reach, reach + 1, size=u.shape[0])
+        dj = rng.integers(-reach, reach + 1, size=u.shape[0])
+        ui, uj = np.divmod(u, side)
+        vi, vj = ui + di, uj + dj
+        ok = (vi >= 0) & (vi < side) & (vj >= 0) & (vj < side) & ((di != 0) | (dj != 0))
+        for a, b in zip(u[ok].tolist(), (vi[ok] * side + vj[ok]).tolist()):
+            key = (a << 32) | b
+            if key in existing:
+                continue
+            existing.add(key)
+            au[k], av[k] = a, b
+            k += 1
+            if k == na:
+                break
+    del_off = np.concatenate([[0], np.cumsum(del_sizes)]).astype(np.int64)
+    add_off = np.concatenate([[0], np.cumsum(add_sizes)]).astype(np.int64)
+    return UpdateStream(du, dv, au, av, del_off, add_off)
+
+
 def write_graph_txt(path: str, g: Graph, weights: bool = True) -> None:
     """Write `u v [w]` lines (the reference's market_big format, weight
     (u+v)%128 as its --weight_num=1 synthesises it)."""

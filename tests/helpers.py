@@ -137,6 +137,13 @@ def heavy_delete_case() -> Case:
     return Case("heavydelete", n, xadj, adj, batches, source=0)
 
 
+def grid_case(side: int = 48, batches: int = 3, size: int = 150) -> Case:
+    """Road-like high-diameter case: a side x side grid, local insertions."""
+    g = gen.grid(side)
+    ups = gen.local_updates(g, side, [size] * batches, [size] * batches, seed=gen.UPDATE_SEED_BASE + 300)
+    return Case(f"grid{side}", g.n, g.xadj, g.adj, [ups.batch(i) for i in range(batches)], source=0)
+
+
 ORACLE_MODE = {"bfs": 0, "sssp": 1, "cc": 2, "sssp_u255": 3}
 
 

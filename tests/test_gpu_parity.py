@@ -13,8 +13,8 @@ import pytest
 
 import oracle
 from coincgraph_b200 import Engine
-from helpers import (ORACLE_MODE, adversarial_case, big_row_case, heavy_delete_case, make_engine, oracle_trace,
-                     rmat_case)
+from helpers import (ORACLE_MODE, adversarial_case, big_row_case, grid_case, heavy_delete_case, make_engine,
+                     oracle_trace, rmat_case)
 
 pytestmark = pytest.mark.gpu
 
@@ -294,3 +294,24 @@ def test_position_index_modes(algo, mode, monkeypatch):
     run_case(heavy_delete_case(), algo, CACHES["zerocopy"])
     run_case_whole_batches(big_row_case(), algo, CACHES["mixed"])
     run_case_whole_batches(rmat_case(11, 3, 400, 400, seed_offset=17), algo, CACHES["resident"])
+
+
+@pytest.mark.parametrize("algo", ["bfs", "sssp", "cc"])
+def test_grid_stream(algo):
+    """High-diameter road-like graph (hundreds of rounds per closure)."""
+    run_case(grid_case(), algo, CACHES["resident"])
+    run_case_whole_batches(grid_case(40, 2, 100), algo, CACHES["zerocopy"])
+
+
+@pytest.mark.parametrize("sweeps", ["0", "1", "4"])
+@pytest.mark.parametrize("algo", ["bfs", "sssp", "cc"])
+def test_local_sweeps(algo, sweeps, monkeypatch):
+    """Block-local sweeps in the push and invalidation closures
+    (CIG_LOCAL_SWEEPS; 0 turns them off) keep values, parent witnesses and
+    rows equal to the oracle's, including local-queue overflow (hub rows)
+    and the grid case."""
+    monkeypatch.setenv("CIG_LOCAL_SWEEPS", sweeps)
+    run_case(grid_case(), algo, CACHES["resident"])
+    run_case(adversarial_case(), algo, CACHES["resident"])
+    run_case_whole_batches(big_row_case(), algo, CACHES["mixed"])
+    run_case_whole_batches(rmat_case(11, 3, 400, 400, seed_offset=18), algo, CACHES["zerocopy"])
