@@ -43,3 +43,24 @@ def test_update_stream_validity(built):
             cur.add(u << 32 | v)
     again = gen.updates(h, [50, 50, 50], [40, 40, 40], seed=gen.UPDATE_SEED_BASE + 7)
     assert np.array_equal(ups.del_v, again.del_v) and np.array_equal(ups.add_u, again.add_u)
+
+
+def test_grid_and_local_updates():
+    """Road-like grid: 4-neighbour rows in east/west/south/north order; update
+    batches delete existing distinct edges and insert new local pairs only."""
+    side = 16
+    g = gen.grid(side)
+    assert g.n == side * side and g.m == 4 * side * (side - 1)
+    row = lambda v: g.adj[int(g.xadj[v]):int(g.xadj[v + 1])].tolist()
+    assert row(0) == [1, side]
+    assert row(side + 1) == [side + 2, side, 2 * side + 1, 1]
+    ups = gen.local_updates(g, side, [20, 20], [30, 30], seed=5)
+    edges = set(zip(np.repeat(np.arange(g.n), np.diff(g.xadj.astype(np.int64))).tolist(), g.adj.tolist()))
+    dels = list(zip(ups.del_u.tolist(), ups.del_v.tolist()))
+    adds = list(zip(ups.add_u.tolist(), ups.add_v.tolist()))
+    assert len(set(dels)) == len(dels) == 40 and all(e in edges for e in dels)
+    assert len(set(adds)) == len(adds) == 60 and not any(e in edges for e in adds)
+    for u, v in adds:
+        assert u != v and abs(u // side - v // side) <= 3 and abs(u % side - v % side) <= 3
+    again = gen.local_updates(g, side, [20, 20], [30, 30], seed=5)
+    assert np.array_equal(again.add_v, ups.add_v) and np.array_equal(again.del_u, ups.del_u)
