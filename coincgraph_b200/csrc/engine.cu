@@ -1389,7 +1389,7 @@ struct cig_handle {
                chunk_map, m, firstpos, status->counters, forward ? seg_hot : nullptr);
         if (ix.keys)
             launch(del_index, persistent_grid(), 256, A.view(), A.desc, sorted, grp, indexed_groups, icount, firstpos,
-                   ix, status);
+                   ix, stats, status);
         prof_end(ps);
         if (prof_on) prof[CIG_STAGE_DEL_SCAN].hits += nd;
         launch(del_apply, grid_for(nd), 256, A.view(), A.desc, sorted, m, firstpos, stats);

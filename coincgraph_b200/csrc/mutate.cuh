@@ -607,20 +607,25 @@ __global__ void del_classify(const RowDesc *desc, const unsigned long long *keys
 // Indexed rows with distinct requests: the first live position of every key
 // from the index; the entry loses one occurrence and, when more remain, moves
 // to the next one (a scan from the deleted position on, rare: parallel
-// edges).  Most groups hold one or two keys, so each lane takes a group of
-// up to kLaneKeys keys alone; larger groups are served by the whole warp.
+// edges).  The tombstone is written here at once (the position is final),
+// and the position is recorded with kApplied set so that del_apply skips
+// it.  Most groups hold one or two keys, so each lane takes a group of up
+// to kLaneKeys keys alone; larger groups are served by the whole warp.
 constexpr uint32_t kLaneKeys = 4;
+constexpr uint32_t kApplied = 0x80000000u;  // firstpos flag: tombstone already written
 
-__device__ __forceinline__ void del_index_key(const AdjView &view, const RowDesc &d, uint32_t u, uint32_t v,
-                                              uint32_t *fp, const PosIndex &ix, Status *st) {
+__device__ __forceinline__ uint32_t del_index_key(const AdjView &view, RowDesc *desc, const RowDesc &d, uint32_t u,
+                                                  uint32_t v, uint32_t *fp, const PosIndex &ix, Status *st) {
     const unsigned long long s = idx_find(ix, (static_cast<unsigned long long>(u) << 32) | v);
-    if (s == ~0ull) return;  // not in the row: a missing delete
+    if (s == ~0ull) return 0u;  // not in the row: a missing delete
     const uint2 e = ix.val[s];
     if (e.y == 0u || e.x >= d.len) {
         if (e.y != 0u) set_error(st, kErrInternal, 0x1d2u);
-        return;
+        return 0u;
     }
-    *fp = e.x;
+    *fp = e.x | kApplied;
+    write_slot(view, d.off + e.x, kTomb);
+    atomicAdd(&desc[u].meta, 1u << 6);
     if (e.y == 1u) {
         ix.val[s] = make_uint2(kInf, 0u);
         ix.keys[s] = kIdxDeleted;
@@ -630,11 +635,14 @@ __device__ __forceinline__ void del_index_key(const AdjView &view, const RowDesc
         if (q >= d.len) set_error(st, kErrInternal, 0x1d3u);
         ix.val[s] = make_uint2(q < d.len ? q : kInf, e.y - 1u);
     }
+    return 1u;
 }
 
-__global__ void del_index(AdjView view, const RowDesc *desc, const unsigned long long *keys, Groups gr,
-                          const uint32_t *list, const uint32_t *count, uint32_t *firstpos, PosIndex ix, Status *st) {
+__global__ void del_index(AdjView view, RowDesc *desc, const unsigned long long *keys, Groups gr,
+                          const uint32_t *list, const uint32_t *count, uint32_t *firstpos, PosIndex ix,
+                          unsigned long long *stats, Status *st) {
     const uint32_t lane = lane_id();
+    uint32_t removed = 0;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t nl = *count;
     for (uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; base < nl; base += warps * 32u) {
@@ -648,7 +656,8 @@ __global__ void del_index(AdjView view, const RowDesc *desc, const unsigned long
         if (i < nl && nk <= kLaneKeys) {
             const uint32_t u = key_src(keys[gs]);
             const RowDesc d = desc[u];
-            for (uint32_t j = 0; j < nk; ++j) del_index_key(view, d, u, key_low(keys[gs + j]), firstpos + gs + j, ix, st);
+            for (uint32_t j = 0; j < nk; ++j)
+                removed += del_index_key(view, desc, d, u, key_low(keys[gs + j]), firstpos + gs + j, ix, st);
         }
         uint32_t todo = __ballot_sync(kFull, i < nl && nk > kLaneKeys);
         while (todo) {
@@ -659,9 +668,10 @@ __global__ void del_index(AdjView view, const RowDesc *desc, const unsigned long
             const uint32_t u = key_src(keys[bs]);
             const RowDesc d = desc[u];
             for (uint32_t j = lane; j < bk; j += 32u)
-                del_index_key(view, d, u, key_low(keys[bs + j]), firstpos + bs + j, ix, st);
+                removed += del_index_key(view, desc, d, u, key_low(keys[bs + j]), firstpos + bs + j, ix, st);
         }
     }
+    if (stats) warp_count(&stats[kCntRemoved], removed);
 }
 
 // After the ordered kernels: the entries of every key of an ordered group on
@@ -848,7 +858,7 @@ __global__ void del_apply(AdjView view, RowDesc *desc, const unsigned long long 
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rounded; i += stride) {
         if (i < m) {
             const uint32_t p = firstpos[i];
-            if (p != kInf) {
+            if (p != kInf && !(p & kApplied)) {
                 const uint32_t u = key_src(keys[i]);
                 write_slot(view, desc[u].off + p, kTomb);
                 atomicAdd(&desc[u].meta, 1u << 6);
