@@ -1505,14 +1505,15 @@ struct cig_handle {
     // Copy host update arrays into the device batch buffers (pinned staging).
     // Host update arrays go through the pinned staging buffer.  Reading the
     // caller's arrays (cold in host DRAM) is what costs: one thread moves
-    // ~6 GB/s, so the calling thread and kStageWorkers persistent workers
+    // ~6 GB/s, so the calling thread and stage_workers persistent workers
     // each copy one part of every array.  The workers spin for kStageSpin
     // after a job before they sleep on a condition variable, so in a stream
     // of batches a call finds them awake (a wake-up from sleep costs about
     // what the split saves).  Then the host-to-device copies are queued on
     // the engine stream.  The previous call's copies have completed (every
     // call ends with a synchronisation), so the buffer is free.
-    static constexpr int kStageWorkers = 3;
+    // Up to 7 workers, leaving one host thread free.
+    const int stage_workers = std::max(1, std::min(7, static_cast<int>(hw_threads()) - 1));
     static constexpr auto kStageSpin = std::chrono::milliseconds(3);
     struct Stager {
         std::vector<std::thread> threads;
@@ -1527,7 +1528,7 @@ struct cig_handle {
     void stager_run(const std::function<void(int)> &job) {
         Stager &S = stager;
         if (S.threads.empty())
-            for (int w = 0; w < kStageWorkers; ++w)
+            for (int w = 0; w < stage_workers; ++w)
                 S.threads.emplace_back([&S, w] {
                     uint64_t seen = 0;
                     for (;;) {
@@ -1546,7 +1547,7 @@ struct cig_handle {
                     }
                 });
         S.job = job;
-        S.pending.store(kStageWorkers, std::memory_order_relaxed);
+        S.pending.store(stage_workers, std::memory_order_relaxed);
         {
             std::lock_guard<std::mutex> lk(S.m);
             S.gen.fetch_add(1, std::memory_order_release);
@@ -1581,7 +1582,7 @@ struct cig_handle {
             }
         };
         if (nd + na >= (1u << 16))
-            stager_run([&](int part) { copy(part, kStageWorkers + 1); });
+            stager_run([&](int part) { copy(part, stage_workers + 1); });
         else
             copy(0, 1);
         uint32_t *dev[4] = {du, dv, au, av};
