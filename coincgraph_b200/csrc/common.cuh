@@ -93,6 +93,8 @@ struct Status {
     uint32_t barrier_count;
     uint32_t barrier_gen;
     unsigned long long counters[40];
+    uint32_t cc_shift;  // CC: depth bits of a value (label << cc_shift | depth); 0 otherwise
+    uint32_t cc_pad;
 };
 
 enum Counter : int {
@@ -226,7 +228,34 @@ __device__ __forceinline__ uint32_t edge_weight(uint32_t u, uint32_t v) {
     return ((u + v) & 127u) + 1u;  // (u+v) mod 2^32 keeps the residue mod 128
 }
 
+__device__ __forceinline__ uint32_t cc_step(uint32_t v, uint32_t shift);
+
+// Value of y relaxed from x with value dx (CC: one more hop from the seed).
+template <int A>
+__device__ __forceinline__ uint32_t relax_value(uint32_t dx, uint32_t x, uint32_t y, uint32_t ccs) {
+    if (A == kCc) return cc_step(dx, ccs);
+    return dx + edge_weight<A>(x, y);
+}
+
 __device__ __forceinline__ uint32_t val_of(unsigned long long s) { return static_cast<uint32_t>(s >> 32); }
+
+// CC values carry a depth below the label: value = label << shift | depth,
+// where depth counts the hops from the component's seed (the vertex whose id
+// is the label) along parents and saturates at the low-bit mask.  The
+// lexicographic minimum (label, depth, parent) makes every unsaturated
+// parent chain strictly shorter towards the seed, so a parent is a rooted
+// witness and a deletion invalidates only the subtree below it; saturated
+// vertices (and shift 0, for graphs of more than 2^31 vertices) fall back to
+// invalidating every equal-label out-neighbour.  Labels (value >> shift) are
+// the reference's values.
+__device__ __forceinline__ uint32_t cc_step(uint32_t v, uint32_t shift) {
+    const uint32_t m = (1u << shift) - 1u;
+    return (v & m) == m ? v : v + 1u;
+}
+__device__ __forceinline__ bool cc_saturated(uint32_t v, uint32_t shift) {
+    const uint32_t m = (1u << shift) - 1u;
+    return (v & m) == m;
+}
 __device__ __forceinline__ uint32_t par_of(unsigned long long s) { return static_cast<uint32_t>(s); }
 __device__ __forceinline__ unsigned long long pack(uint32_t value, uint32_t parent) {
     return (static_cast<unsigned long long>(value) << 32) | parent;

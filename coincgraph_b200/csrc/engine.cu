@@ -823,6 +823,13 @@ struct cig_handle {
         if (bad) throw CigError(CIG_ERR_ARG, "edge destination out of range");
         n = nv;
         source = std::min<uint32_t>(opt.source, n - 1);
+        if (opt.algo == CIG_CC) {
+            // Depth bits below the label (labels are vertex ids < n).
+            uint32_t label_bits = 1;
+            while (label_bits < 32 && (1ull << label_bits) < n) ++label_bits;
+            cc_shift = 32 - label_bits;
+            CK(cudaMemcpy(&status->cc_shift, &cc_shift, sizeof(cc_shift), cudaMemcpyHostToDevice));
+        }
         CK(cudaSetDevice(device));
 
         // Forward arena in pinned mapped host memory.
@@ -1037,7 +1044,7 @@ struct cig_handle {
     // The static solve from scratch (Start, framework.cuh:1151-1182).
     template <int A>
     void static_solve() {
-        launch(init_state<A>, persistent_grid(), 256, state, n, source);
+        launch(init_state<A>, persistent_grid(), 256, state, n, source, cc_shift);
         CK(cudaMemsetAsync(small + kFr, 0, 3 * sizeof(uint32_t), stream));
         if (A == kCc)
             launch(enqueue_all_nonempty, persistent_grid(), 256, fwd.desc, n, frontier(), status);
@@ -1067,6 +1074,7 @@ struct cig_handle {
     }
     bool async_push = false;  // measured equal to the level-synchronous closure on RMAT (CIG_ASYNC_PUSH=1)
     uint32_t local_sweeps = 8;  // block-local hops per closure round (CIG_LOCAL_SWEEPS; 0 = off)
+    uint32_t cc_shift = 0;      // CC: depth bits below the label in a value (also in Status)
     uint32_t *inval_done = nullptr;  // n + 1: vertices the invalidation sweeps expanded
     int async_per_sm = 2;  // worker blocks per SM of the asynchronous closure
     unsigned long long *ring_slot = nullptr;  // ring_cap slots, all zero between closures
@@ -1477,7 +1485,7 @@ struct cig_handle {
                     status);
         prof_end(p);
         p = prof_begin(CIG_STAGE_PULL);
-        launch(reset_affected<A>, persistent_grid(), 256, list, small + kAffTotal, state);
+        launch(reset_affected<A>, persistent_grid(), 256, list, small + kAffTotal, state, cc_shift);
         const BigList pull_big = big_list();
         launch(pull_repair<A>, persistent_grid(), kTpb, rev.view(), state, aff_stamp, epoch, list,
                                                                small + kAffTotal, pull_big, status);
@@ -1736,7 +1744,7 @@ struct cig_handle {
             CK(cudaEventRecord(e[3], stream));
             if (digests) {
                 CK(cudaMemsetAsync(bdig + i, 0, sizeof(unsigned long long), stream));
-                launch(value_digest, persistent_grid(), 256, state, n, bdig + i);
+                launch(value_digest, persistent_grid(), 256, state, n, bdig + i, cc_shift);
             }
             CK(cudaMemcpyAsync(bsnap + 40ull * i, status->counters, 40 * sizeof(unsigned long long),
                                cudaMemcpyDeviceToDevice, stream));
@@ -1805,7 +1813,7 @@ struct cig_handle {
         require_ready();
         if (opt.algo == CIG_PR) throw CigError(CIG_ERR_ARG, "PageRank has no integer values (cig_get_pr)");
         launch(unpack_values, persistent_grid(), 256, state, n, out_values ? tmp_u32 : nullptr,
-                                                              out_parents ? tmp_u32 : nullptr);
+               out_parents ? tmp_u32 : nullptr, cc_shift);
         check_launch();
         CK(cudaMemcpyAsync(out_values ? out_values : out_parents, tmp_u32, n * sizeof(uint32_t),
                            cudaMemcpyDeviceToHost, stream));
@@ -1841,7 +1849,7 @@ struct cig_handle {
         require_ready();
         if (opt.algo == CIG_PR) throw CigError(CIG_ERR_ARG, "PageRank has no integer values");
         CK(cudaMemsetAsync(small64 + 1, 0, sizeof(unsigned long long), stream));
-        launch(value_digest, persistent_grid(), 256, state, n, small64 + 1);
+        launch(value_digest, persistent_grid(), 256, state, n, small64 + 1, cc_shift);
         check_launch();
         unsigned long long h = 0;
         CK(cudaMemcpyAsync(&h, small64 + 1, sizeof(h), cudaMemcpyDeviceToHost, stream));

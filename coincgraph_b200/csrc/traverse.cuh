@@ -45,6 +45,7 @@ struct TagState {
 // 87-127): improve y, and queue it once per round if its value decreased.
 template <int A>
 struct PushOp {
+    uint32_t ccs;  // CC depth bits (Status::cc_shift)
     unsigned long long *state;
     uint32_t *qstamp;
     uint32_t tag;
@@ -56,7 +57,7 @@ struct PushOp {
     __device__ __forceinline__ bool edge(bool valid, uint32_t x, uint32_t dx, uint32_t y) const {
         bool want = false, improved = false;
         if (valid) {
-            const uint32_t nd = dx + edge_weight<A>(x, y);
+            const uint32_t nd = relax_value<A>(dx, x, y, ccs);
             const unsigned long long cand = pack(nd, x);
             if (cand < __ldcg(state + y)) {
                 const unsigned long long old = atomicMin(state + y, cand);
@@ -76,6 +77,7 @@ struct PushOp {
 // do not lead back to the seed.
 template <int A>
 struct InvalOp {
+    uint32_t ccs;
     unsigned long long *state;
     uint32_t *aff_stamp;
     uint32_t epoch;
@@ -89,10 +91,13 @@ struct InvalOp {
         if (valid) {
             const unsigned long long sz = __ldcg(state + z);
             bool dep;
-            if (A == kCc)
-                dep = z != x && val_of(sz) == px && px < z;
-            else
+            if (A == kCc) {
+                const uint32_t vz = val_of(sz);
+                dep = z != x && (par_of(sz) == x || (cc_saturated(vz, ccs) && (vz >> ccs) == (px >> ccs) &&
+                                                     (vz >> ccs) < z));
+            } else {
                 dep = par_of(sz) == x;
+            }
             if (dep && __ldcg(aff_stamp + z) != epoch) want = atomicExch(aff_stamp + z, epoch) != epoch;
         }
         warp_enqueue(want, z, list, count, cap, st);
@@ -106,6 +111,7 @@ struct InvalOp {
 // in-neighbours, which are valid reaching ids.
 template <int A>
 struct PullOp {
+    uint32_t ccs;
     unsigned long long *state;
     const uint32_t *aff_stamp;
     uint32_t epoch;
@@ -115,11 +121,11 @@ struct PullOp {
         unsigned long long cand;
         if (__ldcg(aff_stamp + u) == epoch) {
             if (A != kCc) return false;
-            cand = pack(u, u);
+            cand = pack(cc_step(u << ccs, ccs), u);  // u restarts as its own seed
         } else {
             const uint32_t du = val_of(__ldcg(state + u));
             if (du == kInf) return false;
-            cand = pack(du + edge_weight<A>(u, v), u);
+            cand = pack(relax_value<A>(du, u, v, ccs), u);
         }
         if (cand >= __ldcg(state + v)) return false;
         atomicMin(state + v, cand);
@@ -157,6 +163,7 @@ constexpr uint32_t kSweepItems = 4;  // invalidation sweeps: rounds of at most t
 
 template <int A>
 struct LocalPushOp {
+    uint32_t ccs;
     unsigned long long *state;
     uint32_t *qstamp;
     uint32_t tag;       // membership of the next round's frontier
@@ -170,7 +177,7 @@ struct LocalPushOp {
     __device__ __forceinline__ bool edge(bool valid, uint32_t x, uint32_t dx, uint32_t y) const {
         bool want = false, improved = false;
         if (valid) {
-            const uint32_t nd = dx + edge_weight<A>(x, y);
+            const uint32_t nd = relax_value<A>(dx, x, y, ccs);
             const unsigned long long cand = pack(nd, x);
             if (cand < __ldcg(state + y)) {
                 const unsigned long long old = atomicMin(state + y, cand);
@@ -210,6 +217,7 @@ __global__ void __launch_bounds__(kTpb) push_closure(AdjView fwd, unsigned long 
     // next_tag itself belongs to the seeds queued before this launch.
     const uint32_t tag0 = tags->next_tag + 1;
     const uint32_t sweeps = max_sweeps;
+    const uint32_t ccs = (A == kCc) ? st->cc_shift : 0u;
     uint32_t r = 0;
     for (;; ++r) {
         const uint32_t n_in = ld_volatile(fr.cnt + (r % 3));
@@ -225,7 +233,7 @@ __global__ void __launch_bounds__(kTpb) push_closure(AdjView fwd, unsigned long 
         const uint32_t *in = (r & 1) ? fr.q1 : fr.q0;
         uint32_t *out = (r & 1) ? fr.q0 : fr.q1;
         uint32_t *out_cnt = fr.cnt + ((r + 1) % 3);
-        PushOp<A> op{state, qstamp, tag0 + r, out, out_cnt, fr.cap, st};
+        PushOp<A> op{ccs, state, qstamp, tag0 + r, out, out_cnt, fr.cap, st};
         const Defer df{big.rows, big.cnt + (r % 3), big.cap, big.split};
         if (sweeps) {
             if (threadIdx.x == 0) lq_n[0] = 0;
@@ -249,7 +257,8 @@ __global__ void __launch_bounds__(kTpb) push_closure(AdjView fwd, unsigned long 
             }
             if (sweeps)
                 expand_rows<kTpb>(fwd, has, x, dx, off, deg,
-                                  LocalPushOp<A>{state, qstamp, tag0 + r, out, out_cnt, fr.cap, lq[0], &lq_n[0], st},
+                                  LocalPushOp<A>{ccs, state, qstamp, tag0 + r, out, out_cnt, fr.cap, lq[0], &lq_n[0],
+                                                 st},
                                   sm, cnt, df);
             else
                 expand_rows<kTpb>(fwd, has, x, dx, off, deg, op, sm, cnt, df);
@@ -262,7 +271,8 @@ __global__ void __launch_bounds__(kTpb) push_closure(AdjView fwd, unsigned long 
                 if (nl == 0) break;
                 if (threadIdx.x == 0) lq_n[cur ^ 1u] = 0;
                 __syncthreads();
-                const LocalPushOp<A> lop{state, qstamp, tag0 + r, out, out_cnt, fr.cap, lq[cur ^ 1u], &lq_n[cur ^ 1u], st};
+                const LocalPushOp<A> lop{ccs, state, qstamp, tag0 + r, out, out_cnt, fr.cap, lq[cur ^ 1u],
+                                         &lq_n[cur ^ 1u], st};
                 for (uint32_t base = 0; base < nl; base += kTpb) {
                     const uint32_t i = base + threadIdx.x;
                     bool has = i < nl;
@@ -357,6 +367,7 @@ __device__ __forceinline__ void ring_push(bool want, unsigned long long item, co
 
 template <int A>
 struct PushOpAsync {
+    uint32_t ccs;
     unsigned long long *state;
     uint32_t *qstamp;
     uint32_t mark;  // "queued"
@@ -366,7 +377,7 @@ struct PushOpAsync {
     __device__ __forceinline__ bool edge(bool valid, uint32_t x, uint32_t dx, uint32_t y) const {
         bool want = false, improved = false;
         if (valid) {
-            const uint32_t nd = dx + edge_weight<A>(x, y);
+            const uint32_t nd = relax_value<A>(dx, x, y, ccs);
             const unsigned long long cand = pack(nd, x);
             if (cand < __ldcg(state + y)) {
                 const unsigned long long old = atomicMin(state + y, cand);
@@ -415,7 +426,7 @@ __global__ void __launch_bounds__(kTpb, 4) push_async(AdjView fwd, unsigned long
     const uint32_t lane = lane_id();
     const unsigned long long warps = (gridDim.x * blockDim.x) >> 5;
     const unsigned long long wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const PushOpAsync<A> op{state, qstamp, mark, q, st};
+    const PushOpAsync<A> op{(A == kCc) ? st->cc_shift : 0u, state, qstamp, mark, q, st};
     unsigned long long pos = wid + lane * warps;  // this lane's next ring position
     long long idle_since = 0;
     uint32_t backoff = 32;
@@ -505,6 +516,7 @@ __global__ void __launch_bounds__(kTpb, 4) push_async(AdjView fwd, unsigned long
 // affected list is the same set.
 template <int A>
 struct LocalInvalOp {
+    uint32_t ccs;
     unsigned long long *state;
     uint32_t *aff_stamp;
     uint32_t epoch;
@@ -520,10 +532,13 @@ struct LocalInvalOp {
         if (valid) {
             const unsigned long long sz = __ldcg(state + z);
             bool dep;
-            if (A == kCc)
-                dep = z != x && val_of(sz) == px && px < z;
-            else
+            if (A == kCc) {
+                const uint32_t vz = val_of(sz);
+                dep = z != x && (par_of(sz) == x || (cc_saturated(vz, ccs) && (vz >> ccs) == (px >> ccs) &&
+                                                     (vz >> ccs) < z));
+            } else {
                 dep = par_of(sz) == x;
+            }
             if (dep && __ldcg(aff_stamp + z) != epoch) want = atomicExch(aff_stamp + z, epoch) != epoch;
         }
         const uint32_t mask = __ballot_sync(kFull, want);
@@ -557,6 +572,7 @@ __global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long
     __shared__ uint32_t lq[2][kLocalCap];
     __shared__ uint32_t lq_n[2];
     ExpandCounters c;
+    const uint32_t ccs = (A == kCc) ? st->cc_shift : 0u;
     uint32_t lo = 0, hi = ld_volatile(cnt3 + 0);
     uint32_t r = 0;
     for (;; ++r) {
@@ -569,7 +585,7 @@ __global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long
             cnt3[(r + 2) % 3] = 0;
             big.cnt[(r + 2) % 3] = 0;
         }
-        InvalOp<A> op{state, aff_stamp, epoch, list + hi, cnt3 + ((r + 1) % 3), cap > hi ? cap - hi : 0u, st};
+        InvalOp<A> op{ccs, state, aff_stamp, epoch, list + hi, cnt3 + ((r + 1) % 3), cap > hi ? cap - hi : 0u, st};
         const Defer df{big.rows, big.cnt + (r % 3), big.cap, big.split};
         const uint32_t n_in = hi - lo;
         // Sweeps only for small frontiers (a few items per block): on R-MAT
@@ -596,8 +612,8 @@ __global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long
             }
             if (sweeps)
                 expand_rows<kTpb>(fwd, has, x, px, off, deg,
-                                  LocalInvalOp<A>{state, aff_stamp, epoch, op.list, op.count, op.cap, lq[0], &lq_n[0],
-                                                  st},
+                                  LocalInvalOp<A>{ccs, state, aff_stamp, epoch, op.list, op.count, op.cap, lq[0],
+                                                  &lq_n[0], st},
                                   sm, c, df);
             else
                 expand_rows<kTpb>(fwd, has, x, px, off, deg, op, sm, c, df);
@@ -610,7 +626,7 @@ __global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long
                 if (nl == 0) break;
                 if (threadIdx.x == 0) lq_n[cur ^ 1u] = 0;
                 __syncthreads();
-                const LocalInvalOp<A> lop{state, aff_stamp, epoch, op.list, op.count, op.cap, lq[cur ^ 1u],
+                const LocalInvalOp<A> lop{ccs, state, aff_stamp, epoch, op.list, op.count, op.cap, lq[cur ^ 1u],
                                           &lq_n[cur ^ 1u], st};
                 for (uint32_t base = 0; base < nl; base += kTpb) {
                     const uint32_t i = base + threadIdx.x;
@@ -681,8 +697,10 @@ __global__ void seed_deletions(const uint32_t *du, const uint32_t *dv, uint32_t 
             const unsigned long long sv = __ldcg(state + v);
             bool dep;
             if (A == kCc) {
-                const uint32_t lu = val_of(__ldcg(state + u));
-                dep = u != v && lu == val_of(sv) && val_of(sv) < v;
+                const uint32_t ccs = st->cc_shift;
+                const uint32_t lu = val_of(__ldcg(state + u)) >> ccs;
+                const uint32_t vv = val_of(sv);
+                dep = u != v && (par_of(sv) == u || (cc_saturated(vv, ccs) && lu == (vv >> ccs) && (vv >> ccs) < v));
             } else {
                 dep = par_of(sv) == u && val_of(sv) != kInf;
             }
@@ -695,11 +713,12 @@ __global__ void seed_deletions(const uint32_t *du, const uint32_t *dv, uint32_t 
 // value <- initial value for every invalidated vertex (reset_affected_values,
 // driver.cuh:418-433): unreached for BFS/SSSP, its own id for CC.
 template <int A>
-__global__ void reset_affected(const uint32_t *list, const uint32_t *total, unsigned long long *state) {
+__global__ void reset_affected(const uint32_t *list, const uint32_t *total, unsigned long long *state,
+                               uint32_t ccs) {
     const uint32_t n = *total;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t v = list[i];
-        state[v] = (A == kCc) ? pack(v, kInf) : kInf64;
+        state[v] = (A == kCc) ? pack(v << ccs, kInf) : kInf64;
     }
 }
 
@@ -710,7 +729,7 @@ __global__ void __launch_bounds__(kTpb) pull_repair(AdjView rev, unsigned long l
     __shared__ ExpandSmem<kTpb> sm;
     ExpandCounters c;
     const uint32_t n = *total;
-    PullOp<A> op{state, aff_stamp, epoch};
+    PullOp<A> op{(A == kCc) ? st->cc_shift : 0u, state, aff_stamp, epoch};
     const Defer df{big.rows, big.cnt, big.cap, big.split};
     for (uint32_t base = 0; base < n; base += gridDim.x * kTpb) {
         const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
@@ -734,7 +753,7 @@ template <int A>
 __global__ void __launch_bounds__(kTpb) pull_deferred(AdjView rev, unsigned long long *state, const uint32_t *aff_stamp,
                                                       uint32_t epoch, BigList big, Status *st) {
     ExpandCounters c;
-    PullOp<A> op{state, aff_stamp, epoch};
+    PullOp<A> op{(A == kCc) ? st->cc_shift : 0u, state, aff_stamp, epoch};
     expand_deferred<kTpb>(rev, big.rows, min(*big.cnt, big.cap), op, c);
     flush_counters(st, c, kCntPull);
 }
@@ -773,7 +792,7 @@ __global__ void seed_insertions(const uint32_t *au, const uint32_t *av, uint32_t
         if (u < n && v < n) {
             const uint32_t du = val_of(__ldcg(state + u));
             if (du != kInf) {
-                const uint32_t nd = du + edge_weight<A>(u, v);
+                const uint32_t nd = relax_value<A>(du, u, v, (A == kCc) ? st->cc_shift : 0u);
                 const unsigned long long cand = pack(nd, u);
                 if (cand < __ldcg(state + v)) {
                     const unsigned long long old = atomicMin(state + v, cand);
@@ -788,10 +807,10 @@ __global__ void seed_insertions(const uint32_t *au, const uint32_t *av, uint32_t
 
 // Static-solve initialisation (InitGraph, framework.cuh:991-1041).
 template <int A>
-__global__ void init_state(unsigned long long *state, uint32_t n, uint32_t source) {
+__global__ void init_state(unsigned long long *state, uint32_t n, uint32_t source, uint32_t ccs) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
         if (A == kCc)
-            state[v] = pack(v, kInf);
+            state[v] = pack(v << ccs, kInf);
         else
             state[v] = (v == source) ? pack(0u, kInf) : kInf64;
     }
@@ -807,10 +826,12 @@ __global__ void enqueue_all_nonempty(const RowDesc *desc, uint32_t n, Frontier f
     }
 }
 
-__global__ void unpack_values(const unsigned long long *state, uint32_t n, uint32_t *values, uint32_t *parents) {
+// `ccs` drops the CC depth bits (0 for the other algorithms).
+__global__ void unpack_values(const unsigned long long *state, uint32_t n, uint32_t *values, uint32_t *parents,
+                              uint32_t ccs) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
         const unsigned long long s = state[v];
-        if (values) values[v] = val_of(s);
+        if (values) values[v] = val_of(s) >> ccs;
         if (parents) parents[v] = par_of(s);
     }
 }
@@ -825,10 +846,10 @@ __device__ __forceinline__ unsigned long long digest_mix(unsigned long long z) {
     return z ^ (z >> 31);
 }
 
-__global__ void value_digest(const unsigned long long *state, uint32_t n, unsigned long long *out) {
+__global__ void value_digest(const unsigned long long *state, uint32_t n, unsigned long long *out, uint32_t ccs) {
     unsigned long long acc = 0;
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-        const uint32_t d = val_of(state[v]);
+        const uint32_t d = val_of(state[v]) >> ccs;
         if (d != kInf) acc += digest_mix((static_cast<unsigned long long>(v) << 32) | d);
     }
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
