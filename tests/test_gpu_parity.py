@@ -315,3 +315,48 @@ def test_local_sweeps(algo, sweeps, monkeypatch):
     run_case(adversarial_case(), algo, CACHES["resident"])
     run_case_whole_batches(big_row_case(), algo, CACHES["mixed"])
     run_case_whole_batches(rmat_case(11, 3, 400, 400, seed_offset=18), algo, CACHES["zerocopy"])
+
+
+def _check_cc_witness(eng, case_n, xadj, adj, labels):
+    """Every vertex that is not its own seed has a parent with its label and an
+    edge parent -> vertex, and following parents reaches the seed (the vertex
+    whose id is the label) without revisiting a vertex."""
+    parents = eng.parents()
+    rows = {}
+    for v in range(case_n):
+        if labels[v] == v:
+            continue
+        p = int(parents[v])
+        assert p < case_n and labels[p] == labels[v], f"vertex {v}: parent {p} has another label"
+        if p not in rows:
+            rows[p] = set(adj[int(xadj[p]):int(xadj[p + 1])].tolist())
+        assert v in rows[p], f"vertex {v}: no edge from its parent {p}"
+    for v in range(case_n):
+        seen, x = set(), v
+        while labels[x] != x:
+            assert x not in seen, f"parent cycle through {x}"
+            seen.add(x)
+            x = int(parents[x])
+        assert x == labels[v]
+
+
+@pytest.mark.parametrize("case", ["rmat", "adversarial", "grid"])
+def test_cc_parents_are_rooted_witnesses(case):
+    """CC parents form a forest rooted at each label's seed after the static
+    solve and after every batch (depths never saturate at these sizes), which
+    is what lets a deletion invalidate only the subtree below it."""
+    c = {"rmat": lambda: rmat_case(11, 3, 300, 300, seed_offset=19), "adversarial": adversarial_case,
+         "grid": lambda: grid_case(32, 3, 100)}[case]()
+    g = oracle.Graph(c.n, c.xadj, c.adj)
+    with make_engine("cc", cache_gib=CACHES["resident"]) as eng:
+        eng.load_csr(c.n, c.xadj, c.adj)
+        eng.init()
+        _check_cc_witness(eng, c.n, c.xadj, c.adj, eng.values())
+        for du, dv, au, av in c.batches:
+            g.delete(du, dv)
+            g.add(au, av)
+            eng.apply_batch(du, dv, au, av)
+            labels = eng.values()
+            assert np.array_equal(labels, g.cc())
+            xadj, adj = eng.export_csr()
+            _check_cc_witness(eng, c.n, xadj, adj, labels)
