@@ -262,7 +262,7 @@ int cig_export_csr(cig_handle *h, uint64_t *xadj, uint32_t *adj);
 
 int cig_graph_info_get(cig_handle *h, cig_graph_info *info);
 
-/* Multi-source queries on the current graph (BASELINE workload 3): k BFS
+/* Multi-source queries on the current graph (no reference counterpart): k BFS
  * depths or SSSP distances, k x n row-major, computed with 64-wide bitmask
  * frontiers.  Does not change the maintained state. */
 int cig_query_bfs_multi(cig_handle *h, const uint32_t *sources, uint32_t k, uint32_t *out_depth);
