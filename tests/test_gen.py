@@ -64,3 +64,22 @@ def test_grid_and_local_updates():
         assert u != v and abs(u // side - v // side) <= 3 and abs(u % side - v % side) <= 3
     again = gen.local_updates(g, side, [20, 20], [30, 30], seed=5)
     assert np.array_equal(again.add_v, ups.add_v) and np.array_equal(again.del_u, ups.del_u)
+
+
+def test_bench_road_workload_shapes():
+    """bench.py's road workload: a grid of --side^2 vertices and batches of
+    --batch deletions and insertions (built on the host, no GPU needed)."""
+    import argparse
+    import importlib.util
+    import os
+
+    spec = importlib.util.spec_from_file_location(
+        "bench_mod", os.path.join(os.path.dirname(__file__), "..", "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    args = argparse.Namespace(workload="road", side=20, batch=15, scale=24, edge_factor=16)
+    g, ups, setup = bench.make_workload(args, 3)
+    assert g.n == 400 and ups.batches == 3 and set(setup) == {"gen_graph_s", "gen_updates_s"}
+    for i in range(3):
+        du, dv, au, av = ups.batch(i)
+        assert len(du) == len(dv) == len(au) == len(av) == 15
