@@ -828,6 +828,10 @@ struct cig_handle {
             uint32_t label_bits = 1;
             while (label_bits < 32 && (1ull << label_bits) < n) ++label_bits;
             cc_shift = 32 - label_bits;
+            // CIG_CC_DEPTH_BITS caps the depth field (0 keeps the equal-label
+            // rule everywhere; small values make saturation common).
+            if (const char *e = std::getenv("CIG_CC_DEPTH_BITS"))
+                cc_shift = std::min<uint32_t>(cc_shift, static_cast<uint32_t>(std::max(0, std::atoi(e))));
             CK(cudaMemcpy(&status->cc_shift, &cc_shift, sizeof(cc_shift), cudaMemcpyHostToDevice));
         }
         CK(cudaSetDevice(device));

@@ -360,3 +360,15 @@ def test_cc_parents_are_rooted_witnesses(case):
             assert np.array_equal(labels, g.cc())
             xadj, adj = eng.export_csr()
             _check_cc_witness(eng, c.n, xadj, adj, labels)
+
+
+@pytest.mark.parametrize("bits", ["0", "2"])
+def test_cc_saturated_depths(bits, monkeypatch):
+    """With the CC depth field capped (CIG_CC_DEPTH_BITS: 0 bits, or 2 bits so
+    that depths saturate at 3 hops), saturated vertices fall back to the
+    equal-label invalidation rule; labels and rows still equal the oracle's."""
+    monkeypatch.setenv("CIG_CC_DEPTH_BITS", bits)
+    run_case(rmat_case(11, 3, 300, 300, seed_offset=20), "cc", CACHES["resident"])
+    run_case(adversarial_case(), "cc", CACHES["resident"])
+    run_case(grid_case(24, 3, 80), "cc", CACHES["resident"])
+    run_case_whole_batches(rmat_case(10, 3, 200, 200, seed_offset=21, symmetric=True), "cc", CACHES["mixed"])
