@@ -54,6 +54,7 @@ def parse_args():
     p.add_argument("--cache", type=float, default=1.0, help="HBM edge-cache budget, GiB")
     p.add_argument("--algo", default="sssp", choices=["bfs", "sssp", "cc"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-parity", action="store_true", help="skip the oracle replay after the timed region")
     p.add_argument("--ref-budget-s", type=float, default=150.0,
                    help="reference arm: stop timing after this much CPU time")
     p.add_argument("--workload", default="stream",
@@ -238,6 +239,49 @@ def traffic_ratio(kernel):
     return None, None
 
 
+def stream_config(args, g):
+    """The workload keys both arms report (identical dicts for one run)."""
+    if args.workload == "stream" and args.scale == 24 and args.batch == 100_000 and args.algo == "sssp":
+        name = WORKLOAD
+    else:
+        name = (f"incremental {args.algo.upper()}, "
+                + (f"road-like grid {args.side}x{args.side}" if args.workload == "road" else
+                   f"RMAT s{args.scale} ef{args.edge_factor}")
+                + f", cache {args.cache} GiB, {args.batch} del + {args.batch} ins per batch")
+    return {"workload": name, "algo": args.algo, "scale": args.scale if args.workload != "road" else None,
+            "vertices": g.n, "edges": g.m, "batch": args.batch, "cache_gib": args.cache, "source": 0,
+            "l2": "GPU arm: L2 flushed between steps (256 MiB write)", "parallelism": "replicas"}
+
+
+def oracle_parity(g, ups, applied, eng, args):
+    """Replay every batch the engine applied, in order, on the oracle (the
+    CPU restatement of the reference's row mutation and --check solvers),
+    outside every timer, and compare the engine's final values and rows with
+    the oracle's exactly."""
+    import oracle
+
+    t0 = time.perf_counter()
+    og = oracle.Graph(g.n, g.xadj, g.adj)
+    missing = 0
+    for i in range(applied):
+        du, dv, au, av = ups.batch(i)
+        missing += og.delete(du, dv)
+        og.add(au, av)
+    mode = {"bfs": oracle.BFS, "sssp": oracle.SSSP, "cc": oracle.CC}[args.algo]
+    want = og.cc() if args.algo == "cc" else og.sssp(0, mode)
+    got = eng.values()
+    diff = int(np.count_nonzero(got != want))
+    xadj, adj = eng.export_csr()
+    xo, ao = og.export()
+    rows_ok = bool(np.array_equal(xadj, xo) and np.array_equal(adj, ao))
+    del og, xadj, adj, xo, ao
+    return {"values_equal": diff == 0, "values_differing": diff, "rows_equal": rows_ok,
+            "batches_replayed": applied, "reached": int(np.count_nonzero(want != oracle.INF)),
+            "oracle": f"oracle/ FIFO label-correcting {args.algo} (restated reference --check) after replaying "
+                      "every applied batch on the restated chunk-store mutation",
+            "seconds": round(time.perf_counter() - t0, 1)}
+
+
 def cpu_baseline(g, ups, args, batch_index):
     """Reference CPU path on one batch: its SourceLocalChunkStore maintenance
     (compiled from the reference sources) + the FIFO recompute of --check."""
@@ -319,10 +363,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": len(times), "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": (f"incremental {args.algo.upper()}, road-like grid {args.side}x{args.side}, "
-                                f"{args.batch} del + {args.batch} ins per batch") if args.workload == "road" else
-                   WORKLOAD if args.scale == 24 else f"{WORKLOAD} (scale {args.scale})",
-                   "scale": args.scale, "batch": args.batch, "algo": args.algo, "setup": setup},
+        "config": stream_config(args, g), "setup": setup,
         "p50_ms": statistics.median(times) * 1e3, "p99_ms": float(np.percentile(np.array(times) * 1e3, 99)),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "reference" if have_ref else "port",
                          "sample": (f"{len(times)} timed batches (of {args.steps} requested, CPU-time budget "
@@ -445,6 +486,12 @@ def run_ours(args):
             roofline["traffic_source"] = (f"ncu dram__bytes_read+write of {roofline['kernel']} on {src}, "
                                           f"{ratio:.3f} x algorithmic HBM bytes, scaled to this launch "
                                           f"(profiles/traffic.md)")
+    parity = None
+    if rank == 0 and not args.no_parity:
+        try:
+            parity = oracle_parity(g, ups, args.warmup + 2 * args.steps, eng, args)
+        except Exception as e:  # reported in the line, not fatal
+            parity = {"values_equal": False, "rows_equal": False, "error": str(e)}
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -457,15 +504,10 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": WORKLOAD if args.workload == "stream" and args.scale == 24 and args.batch == 100_000
-                       else f"incremental {args.algo.upper()}, "
-                       + (f"road-like grid {args.side}x{args.side}" if args.workload == "road" else
-                          f"RMAT s{args.scale} ef{args.edge_factor}")
-                       + f", cache {args.cache} GiB, {args.batch} del + {args.batch} ins per batch",
-                       "algo": args.algo, "vertices": g.n, "edges": g.m, "cache_gib": args.cache,
-                       "segments_resident": info["segments_resident"], "segments_total": info["segments_total"],
-                       "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
-                       "setup": setup},
+            "config": stream_config(args, g), "setup": setup,
+            "engine": {"segments_resident": info["segments_resident"], "segments_total": info["segments_total"]},
+            "parity": parity["values_equal"] and parity["rows_equal"] if parity else None,
+            "parity_detail": parity,
             "gteps": edges / total_s / 1e9 * world if total_s else None,
             "p50_ms": statistics.median(ms), "p99_ms": float(np.percentile(ms, 99)),
             "updates_per_s": value * 2 * args.batch,

@@ -140,6 +140,7 @@ static void define_flags() {
     def("update_size", 's', "", "A file with the per-batch `adds dels` sizes");
     def("cache", 'd', "4", "HBM edge-cache budget in GiB of 4-byte slots");
     def("cache_compat", 'b', "false", "map --cache through the reference's slot table (graph_datum.cuh:158-170)");
+    def("index_budget", 'd', "0", "device GiB for the two position-index tables (0: a quarter of free memory each)");
     def("top_ranks", 'i', "10", "(accepted, no effect)");
     def("print_ranks", 'b', "false", "(accepted, no effect)");
     def("device", 'i', "0", "CUDA device ordinal");
@@ -674,6 +675,7 @@ static bool run() {
     o.device = static_cast<int32_t>(I("device"));
     o.cache_gib = D("cache");
     o.cache_compat = B("cache_compat") ? 1 : 0;
+    o.index_budget_gib = D("index_budget");
 #if defined(CIG_TOOL_PR)
     o.pr_epsilon = eps;
     o.pr_max_rounds = static_cast<int32_t>(max_rounds);

@@ -192,6 +192,7 @@ enum SmallIdx : int {
     kInvalDone = 22,     // vertices expanded by the invalidation closure's local sweeps
     kGaF = 18,  // addition-phase group counts of a presorted batch
     kGaR = 19,
+    kEpoch = 23,  // batch epoch of the traversal algorithms (aff_stamp marker)
     kSmallCount = 24
 };
 
@@ -345,7 +346,11 @@ struct cig_handle {
         CK(cudaStreamSynchronize(stream));
         size_t fr = 0, tot = 0;
         CK(cudaMemGetInfo(&fr, &tot));
-        const uint64_t share = (fr + b.cap * (sizeof(unsigned long long) + sizeof(uint2))) / 4;
+        // Each table may take half of --index_budget, or else a quarter of
+        // the free device memory (counting the table it replaces).
+        const uint64_t share = opt.index_budget_gib > 0
+                                   ? static_cast<uint64_t>(opt.index_budget_gib * 1073741824.0 / 2.0)
+                                   : (fr + b.cap * (sizeof(unsigned long long) + sizeof(uint2))) / 4;
         uint64_t entries = 0, cap = 0;
         uint32_t cls = 64;
         for (uint32_t c = 63; c + 1 > index_cls; --c) {
@@ -424,6 +429,13 @@ struct cig_handle {
     cig_stage_profile prof[CIG_STAGE_COUNT] = {};
 
     cudaEvent_t take_event() {
+        if (capturing) {
+            // A captured graph records its own events on every replay.
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            capture_events.push_back(e);
+            return e;
+        }
         if (ev_used == ev_pool.size()) {
             cudaEvent_t e;
             CK(cudaEventCreate(&e));
@@ -431,17 +443,25 @@ struct cig_handle {
         }
         return ev_pool[ev_used++];
     }
+    // Record an event on the engine stream; under stream capture it becomes
+    // an event-record node of the graph (recorded at every replay).
+    void rec(cudaEvent_t e) {
+        if (capturing)
+            CK(cudaEventRecordWithFlags(e, stream, cudaEventRecordExternal));
+        else
+            CK(cudaEventRecord(e, stream));
+    }
     int prof_begin(int stage) {
         if (!prof_on) return -1;
         cudaEvent_t a = take_event();
-        CK(cudaEventRecord(a, stream));
+        rec(a);
         prof_pending.push_back({stage, a, nullptr});
         return static_cast<int>(prof_pending.size()) - 1;
     }
     void prof_end(int idx) {
         if (idx < 0) return;
         cudaEvent_t b = take_event();
-        CK(cudaEventRecord(b, stream));
+        rec(b);
         prof_pending[idx].b = b;
     }
     void prof_resolve() {
@@ -517,8 +537,24 @@ struct cig_handle {
     void launch_coop(void (*kernel)(P...), int tpb, typename Identity<P>::type... args) {
         void *argv[] = {static_cast<void *>(&args)...};
         const int blocks = coop_blocks(kernel, tpb);
-        CK(cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(kernel), dim3(blocks), dim3(tpb), argv, 0,
-                                       stream));
+        if (capturing) {
+            // Captured as a kernel node with the cooperative attribute: the
+            // graph launch keeps the co-residency guarantee of the grid.
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeCooperative;
+            attr[0].val.cooperative = 1;
+            cudaLaunchConfig_t cfg{};
+            cfg.gridDim = dim3(blocks);
+            cfg.blockDim = dim3(tpb);
+            cfg.dynamicSmemBytes = 0;
+            cfg.stream = stream;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            CK(cudaLaunchKernelExC(&cfg, reinterpret_cast<const void *>(kernel), argv));
+        } else {
+            CK(cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(kernel), dim3(blocks), dim3(tpb), argv, 0,
+                                           stream));
+        }
         ++n_launch;
     }
 
@@ -531,6 +567,142 @@ struct cig_handle {
     }
 
     void check_launch() { CK(cudaGetLastError()); }
+
+    // ------------------------------------------------------------ CUDA graphs of the batch path
+    // A batch (or one phase) of the traversal algorithms is a fixed chain of
+    // ~60 launches and memsets on the engine stream whose arguments depend
+    // only on the batch shape (deletions, insertions) and on device buffers
+    // that stay put between reallocations; everything that changes per batch
+    // (epoch, tags, counts) lives on the device.  So the chain is captured
+    // once per shape into a CUDA graph and replayed with one launch.  A shape
+    // is captured the second time it is seen (uneven streams of one-off
+    // sizes stay on direct launches).  Anything that reallocates a captured
+    // buffer or changes a launch shape bumps `graph_gen`, which retires every
+    // graph.  Host decisions that used to sit inside the chain run before
+    // the replay: position-index upkeep (index_upkeep) and the scan-chunk map
+    // size (reserve_chunk_map).  CIG_GRAPHS=0 turns graphs off.
+    struct BatchGraph {
+        int kind = 0;  // 0 whole batch, 1 deletion phase, 2 insertion phase
+        uint64_t nd = 0, na = 0, gen = 0, last_use = 0;
+        bool prof = false;
+        cudaGraphExec_t exec = nullptr;
+        uint64_t launches = 0;
+        std::vector<ProfRec> prof_recs;
+        std::vector<cudaEvent_t> events;
+    };
+    std::vector<BatchGraph> graphs;
+    std::vector<std::pair<int, std::pair<uint64_t, uint64_t>>> shapes_seen;
+    std::vector<cudaEvent_t> capture_events;
+    bool use_graphs = true;
+    bool capturing = false;
+    uint64_t graph_gen = 1, graph_clock = 0;
+    uint64_t graph_replays = 0, graph_captures = 0;
+    static constexpr size_t kMaxGraphs = 8;
+
+    static void release_graph(BatchGraph &g) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        for (auto e : g.events) cudaEventDestroy(e);
+        g.exec = nullptr;
+        g.events.clear();
+    }
+    void drop_graphs() {
+        for (auto &g : graphs) release_graph(g);
+        graphs.clear();
+        shapes_seen.clear();
+    }
+    void retire_graphs() { ++graph_gen; }
+
+    // Run `body` (the launches of one batch or phase of shape kind/nd/na on
+    // the engine stream) through the graph cache.
+    template <class F>
+    void run_graphed(int kind, uint64_t nd, uint64_t na, F body) {
+        if (!use_graphs) {
+            body();
+            return;
+        }
+        for (auto &g : graphs) {
+            if (g.kind == kind && g.nd == nd && g.na == na && g.gen == graph_gen && g.prof == prof_on) {
+                CK(cudaGraphLaunch(g.exec, stream));
+                n_launch += g.launches;
+                g.last_use = ++graph_clock;
+                ++graph_replays;
+                if (prof_on) prof_pending.insert(prof_pending.end(), g.prof_recs.begin(), g.prof_recs.end());
+                return;
+            }
+        }
+        const std::pair<int, std::pair<uint64_t, uint64_t>> shape{kind, {nd, na}};
+        if (std::find(shapes_seen.begin(), shapes_seen.end(), shape) == shapes_seen.end()) {
+            if (shapes_seen.size() >= 64) shapes_seen.erase(shapes_seen.begin());
+            shapes_seen.push_back(shape);
+            body();
+            return;
+        }
+        // Second sighting of this shape: capture it, then replay it.
+        for (auto it = graphs.begin(); it != graphs.end();) {
+            if (it->gen != graph_gen) {
+                release_graph(*it);
+                it = graphs.erase(it);
+            } else {
+                ++it;
+            }
+        }
+        if (graphs.size() >= kMaxGraphs) {
+            auto lru = std::min_element(graphs.begin(), graphs.end(),
+                                        [](const BatchGraph &a, const BatchGraph &b) { return a.last_use < b.last_use; });
+            release_graph(*lru);
+            graphs.erase(lru);
+        }
+        BatchGraph g;
+        g.kind = kind;
+        g.nd = nd;
+        g.na = na;
+        g.gen = graph_gen;
+        g.prof = prof_on;
+        const uint64_t l0 = n_launch;
+        const size_t p0 = prof_pending.size();
+        const bool presorted0 = presorted;
+        capture_events.clear();
+        CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        capturing = true;
+        cudaGraph_t graph = nullptr;
+        try {
+            body();
+        } catch (...) {
+            capturing = false;
+            cudaStreamEndCapture(stream, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            for (auto e : capture_events) cudaEventDestroy(e);
+            capture_events.clear();
+            prof_pending.resize(p0);
+            n_launch = l0;
+            throw;
+        }
+        capturing = false;
+        const cudaError_t ec = cudaStreamEndCapture(stream, &graph);
+        cudaError_t ei = cudaErrorUnknown;
+        if (ec == cudaSuccess) ei = cudaGraphInstantiateWithFlags(&g.exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        g.events.swap(capture_events);
+        if (ec != cudaSuccess || ei != cudaSuccess) {
+            release_graph(g);
+            cudaGetLastError();
+            throw CigError(CIG_ERR_DEVICE, std::string("batch graph capture failed: ") +
+                                               cudaGetErrorString(ec != cudaSuccess ? ec : ei));
+        }
+        g.launches = n_launch - l0;
+        n_launch = l0;
+        g.prof_recs.assign(prof_pending.begin() + p0, prof_pending.end());
+        prof_pending.resize(p0);
+        presorted = presorted0;
+        ++graph_captures;
+        graphs.push_back(std::move(g));
+        BatchGraph &r = graphs.back();
+        CK(cudaGraphLaunch(r.exec, stream));
+        n_launch += r.launches;
+        r.last_use = ++graph_clock;
+        if (prof_on) prof_pending.insert(prof_pending.end(), r.prof_recs.begin(), r.prof_recs.end());
+    }
 
     uint64_t launch_mark = 0;
 
@@ -608,14 +780,13 @@ struct cig_handle {
         pr64 = (opt.flags & CIG_FLAG_PR_FP64) != 0;
         if (const char *e = std::getenv("CIG_COOP_BLOCKS_PER_SM")) tune.per_sm = std::max(1, std::atoi(e));
         if (const char *e = std::getenv("CIG_SPLIT_DEG")) tune.split = std::max(32, std::atoi(e));
-        if (const char *e = std::getenv("CIG_ASYNC_PUSH")) async_push = std::atoi(e) != 0;
         if (const char *e = std::getenv("CIG_LOCAL_SWEEPS")) local_sweeps = static_cast<uint32_t>(std::max(0, std::atoi(e)));
+        if (const char *e = std::getenv("CIG_GRAPHS")) use_graphs = std::atoi(e) != 0;
         if (const char *e = std::getenv("CIG_POS_INDEX")) use_index = std::atoi(e) != 0;
         if (const char *e = std::getenv("CIG_POS_INDEX_CLS")) index_cls = static_cast<uint32_t>(std::atoi(e));
         if (const char *e = std::getenv("CIG_POS_INDEX_HEADROOM"))
             index_headroom = std::max<uint64_t>(64, std::strtoull(e, nullptr, 10));
         if (const char *e = std::getenv("CIG_POS_INDEX_SPARE")) index_spare = std::max(0.0, std::atof(e));
-        if (const char *e = std::getenv("CIG_ASYNC_PER_SM")) async_per_sm = std::max(1, std::atoi(e));
         if (const char *e = std::getenv("CIG_PULL_ON")) tune.pull_on = static_cast<uint32_t>(std::max(0, std::atoi(e)));
         if (const char *e = std::getenv("CIG_PULL_OFF")) tune.pull_off = static_cast<uint32_t>(std::max(1, std::atoi(e)));
     }
@@ -624,6 +795,7 @@ struct cig_handle {
         stager_stop();
         cudaSetDevice(device);
         if (stream) cudaStreamSynchronize(stream);
+        drop_graphs();
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
         for (auto &e : ev_pool) cudaEventDestroy(e);
@@ -646,8 +818,6 @@ struct cig_handle {
         dfree(seg_ctl);
         dfree(state);
         dfree(qstamp);
-        dfree(ring_slot);
-        dfree(ring_ctr);
         dfree(aff_stamp);
         dfree(q0);
         dfree(q1);
@@ -784,6 +954,7 @@ struct cig_handle {
         CK(cudaMalloc(&cub, std::max<size_t>(bytes, 16)));
         CK(cudaHostAlloc(reinterpret_cast<void **>(&stage), 4 * cap * sizeof(uint32_t), cudaHostAllocDefault));
         bcap = cap;
+        retire_graphs();
     }
 
     int key_end_bit() const {
@@ -970,12 +1141,6 @@ struct cig_handle {
         } else {
             dmalloc(state, n);
             dmalloc(qstamp, n);
-            // vertices + chunk items of long rows (at most one chunk per kAsyncChunk arena slots)
-            ring_cap = static_cast<uint32_t>(std::min<uint64_t>(0xFFFFFFF0ull, static_cast<uint64_t>(n) + 1 +
-                                                                 fwd.seg_total * (kSegEdges / kAsyncChunk)));
-            dmalloc(ring_slot, ring_cap);
-            CK(cudaMemset(ring_slot, 0, static_cast<size_t>(ring_cap) * sizeof(unsigned long long)));
-            dmalloc(ring_ctr, kRingCtrWords);
             dmalloc(aff_stamp, n);
             dmalloc(list, n + 1);
             CK(cudaMemset(qstamp, 0, n * sizeof(uint32_t)));
@@ -1058,32 +1223,18 @@ struct cig_handle {
         run_push<A>();
     }
 
-    // Push closure from the queued seeds: level-synchronous (cooperative,
-    // grid barriers) for the static solve, asynchronous (ring worklist, no
-    // barriers) for the small frontiers of incremental batches.
+    // Push closure from the queued seeds (persistent, cooperative, bounded
+    // grid barriers), for the static solve and for incremental batches.
     template <int A>
-    void run_push(bool incremental = false) {
+    void run_push() {
         const int p = prof_begin(CIG_STAGE_PUSH);
-        if (incremental && async_push) {
-            CK(cudaMemsetAsync(ring_ctr, 0, kRingCtrWords * sizeof(unsigned long long), stream));
-            const AsyncRing ring{ring_slot, ring_ctr, ring_cap};
-            launch(async_seed, persistent_grid(), 256, q0, small + kFr, qstamp, tags, ring, status);
-            launch(push_async<A>, sms * async_per_sm, kTpb, fwd.view(), state, qstamp, tags, ring, seg_hot, status);
-            launch(advance_tag, 1, 1, tags, 2u);
-        } else {
-            launch_coop(push_closure<A>, kTpb, fwd.view(), state, qstamp, tags, frontier(), big_list(), n + 2,
-                        local_sweeps, seg_hot, status);
-        }
+        launch_coop(push_closure<A>, kTpb, fwd.view(), state, qstamp, tags, frontier(), big_list(), n + 2,
+                    local_sweeps, seg_hot, status);
         prof_end(p);
     }
-    bool async_push = false;  // measured equal to the level-synchronous closure on RMAT (CIG_ASYNC_PUSH=1)
     uint32_t local_sweeps = 8;  // block-local hops per closure round (CIG_LOCAL_SWEEPS; 0 = off)
     uint32_t cc_shift = 0;      // CC: depth bits below the label in a value (also in Status)
     uint32_t *inval_done = nullptr;  // n + 1: vertices the invalidation sweeps expanded
-    int async_per_sm = 2;  // worker blocks per SM of the asynchronous closure
-    unsigned long long *ring_slot = nullptr;  // ring_cap slots, all zero between closures
-    uint32_t ring_cap = 0;
-    unsigned long long *ring_ctr = nullptr;  // tail, head, done
 
     // ------------------------------------------------------------ PR
     template <class T>
@@ -1248,6 +1399,7 @@ struct cig_handle {
         }
         tune.pull_on = pull_best;
         tune.pull_off = pull_best * 2;
+        retire_graphs();  // launch shapes changed
         if (res) {
             std::memset(res, 0, sizeof(*res));
             res->blocks_per_sm = best.per_sm;
@@ -1341,6 +1493,44 @@ struct cig_handle {
         return true;
     }
 
+    // Scan-chunk map of a deletion phase: at most one chunk per 512 arena
+    // slots plus one per group.  Sized before the phase's launches are
+    // queued (or captured).
+    void reserve_chunk_map(uint64_t nd) {
+        const uint64_t need = std::max(fwd.seg_total, rev.seg_total) * (kSegEdges / kDelChunk) + nd + 1;
+        if (need <= chunk_map_cap) return;
+        if (capturing) throw CigError(CIG_ERR_DEVICE, "internal: scan-chunk map grows under capture");
+        CK(cudaStreamSynchronize(stream));
+        dfree(chunk_map);
+        dmalloc(chunk_map, need);
+        chunk_map_cap = need;
+        retire_graphs();
+    }
+
+    // Position-index upkeep before an insertion phase of `na` additions: a
+    // table is rebuilt once its load factor could pass one half (every
+    // addition may add a key).  Runs before the phase's launches are queued
+    // or replayed; a rebuild synchronises and retires the captured graphs.
+    void index_upkeep(uint64_t na) {
+        if (!na) return;
+        for (int a = 0; a < 2; ++a) {
+            IndexBuf &b = ixb[a];
+            if (!b.cap) continue;
+            b.inserted += na;
+            if (2 * (b.entries + b.inserted) > b.cap) {
+                const int pi = prof_begin(CIG_STAGE_INDEX);
+                build_index(a == 0 ? fwd : rev, a == 0);
+                prof_end(pi);
+                retire_graphs();
+            }
+        }
+    }
+
+    // Host-side accounting of a deletion phase (kept out of captured code).
+    void note_delete_phase(uint64_t nd) {
+        if (prof_on && nd) prof[CIG_STAGE_DEL_SCAN].hits += 2 * nd;
+    }
+
     void mutate_delete_arena(DevArena &A, const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd, bool forward,
                              bool with_stats) {
         if (nd == 0) return;
@@ -1385,16 +1575,7 @@ struct cig_handle {
             size_t bytes = cub_bytes;
             CK(cub::DeviceScan::InclusiveSum(cub, bytes, chunks, chunk_end, static_cast<int>(nd), stream));
         }
-        {
-            // Chunks of a phase: at most one per 512 arena slots plus one per group.
-            const uint64_t need = A.seg_total * (kSegEdges / kDelChunk) + nd + 1;
-            if (need > chunk_map_cap) {
-                CK(cudaStreamSynchronize(stream));
-                dfree(chunk_map);
-                dmalloc(chunk_map, need);
-                chunk_map_cap = need;
-            }
-        }
+        reserve_chunk_map(nd);
         launch(del_chunk_map, persistent_grid(), 256, grp, chunk_end, chunk_map);
         const int ps = prof_begin(CIG_STAGE_DEL_SCAN);
         launch(del_scan, sms * del_scan_blocks_per_sm(), kMutWarps * 32, A.view(), A.desc, sorted, grp, chunk_end,
@@ -1403,7 +1584,6 @@ struct cig_handle {
             launch(del_index, persistent_grid(), 256, A.view(), A.desc, sorted, grp, indexed_groups, icount, firstpos,
                    ix, stats, status);
         prof_end(ps);
-        if (prof_on) prof[CIG_STAGE_DEL_SCAN].hits += nd;
         launch(del_apply, grid_for(nd), 256, A.view(), A.desc, sorted, m, firstpos, stats);
         launch(del_finish, persistent_grid(), 256, A.desc, sorted, grp, gtype, firstpos, compact, ccount, stats);
         // Ordered path: rows with repeated requests for a destination.
@@ -1446,15 +1626,6 @@ struct cig_handle {
         CK(cudaMemsetAsync(bcount, 0, sizeof(uint32_t), stream));
         prof_end(p);
         p = prof_begin(forward ? CIG_STAGE_ADD : CIG_STAGE_ADD_REV);
-        if (ixb[forward ? 0 : 1].cap) {
-            IndexBuf &b = ixb[forward ? 0 : 1];
-            b.inserted += na;
-            if (2 * (b.entries + b.inserted) > b.cap) {
-                const int pi = prof_begin(CIG_STAGE_INDEX);
-                build_index(A, forward);
-                prof_end(pi);
-            }
-        }
         launch(plan_add, persistent_grid(), 256, A.desc, sorted, grp, plan, A.alloc);
         launch(alloc_classes, 1, 64, A.alloc, status);
         if (forward && refresh) launch(seg_assign_new, 1, 32, seg_table(), &A.alloc->seg_bump, status);
@@ -1472,32 +1643,32 @@ struct cig_handle {
     // ------------------------------------------------------------ batches
     template <int A>
     void delete_phase_dev(const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd) {
-        ++epoch;
-        CK(cudaMemsetAsync(small + kFr, 0, 6 * sizeof(uint32_t), stream));  // frontier + affected counters
+        const uint32_t *ep = small + kEpoch;
+        launch(phase_begin, 1, 32, small + kEpoch, small + kFr, 6u);  // frontier + affected counters
         int p = prof_begin(CIG_STAGE_SEED);
         if (nd)
             launch(seed_deletions<A>, grid_for(nd), 256, d_du, d_dv, static_cast<uint32_t>(nd), n, state,
-                                                                aff_stamp, epoch, list, small + kAff, n + 1, status);
+                                                                aff_stamp, ep, list, small + kAff, n + 1, status);
         prof_end(p);
         check_launch();
         mutate_delete_arena(fwd, d_du, d_dv, nd, true, true);
         mutate_delete_arena(rev, d_du, d_dv, nd, false, false);
         p = prof_begin(CIG_STAGE_INVAL);
         if (local_sweeps) CK(cudaMemsetAsync(small + kInvalDone, 0, sizeof(uint32_t), stream));
-        launch_coop(inval_closure<A>, kTpb, fwd.view(), state, aff_stamp, epoch, list, small + kAff, n + 1,
+        launch_coop(inval_closure<A>, kTpb, fwd.view(), state, aff_stamp, ep, list, small + kAff, n + 1,
                     big_list(), n + 2, local_sweeps, inval_done, small + kInvalDone, small + kAffTotal, seg_hot,
                     status);
         prof_end(p);
         p = prof_begin(CIG_STAGE_PULL);
         launch(reset_affected<A>, persistent_grid(), 256, list, small + kAffTotal, state, cc_shift);
         const BigList pull_big = big_list();
-        launch(pull_repair<A>, persistent_grid(), kTpb, rev.view(), state, aff_stamp, epoch, list,
+        launch(pull_repair<A>, persistent_grid(), kTpb, rev.view(), state, aff_stamp, ep, list,
                                                                small + kAffTotal, pull_big, status);
-        launch(pull_deferred<A>, persistent_grid(), kTpb, rev.view(), state, aff_stamp, epoch, pull_big, status);
+        launch(pull_deferred<A>, persistent_grid(), kTpb, rev.view(), state, aff_stamp, ep, pull_big, status);
         launch(enqueue_affected<A>, persistent_grid(), 256, list, small + kAffTotal, state, frontier(), status);
         prof_end(p);
         check_launch();
-        run_push<A>(true);
+        run_push<A>();
     }
 
     template <int A>
@@ -1511,7 +1682,7 @@ struct cig_handle {
                                                                  qstamp, tags, frontier(), status);
         prof_end(p);
         check_launch();
-        run_push<A>(true);
+        run_push<A>();
     }
 
     // Copy host update arrays into the device batch buffers (pinned staging).
@@ -1615,7 +1786,11 @@ struct cig_handle {
         reset_counters();
         CK(cudaEventRecord(ev[0], stream));
         stage_batch(hu, hv, nd, nullptr, nullptr, 0);
-        dispatch([&](auto tag) { delete_phase_dev<decltype(tag)::value>(du, dv, nd); });
+        note_delete_phase(nd);
+        reserve_chunk_map(nd);
+        dispatch([&](auto tag) {
+            run_graphed(1, nd, 0, [&] { delete_phase_dev<decltype(tag)::value>(du, dv, nd); });
+        });
         CK(cudaEventRecord(ev[1], stream));
         finish();
         fill_stats(s, nd, 0, true, false);
@@ -1628,12 +1803,62 @@ struct cig_handle {
         reset_counters();
         CK(cudaEventRecord(ev[1], stream));
         stage_batch(nullptr, nullptr, 0, hu, hv, na);
-        dispatch([&](auto tag) { insert_phase_dev<decltype(tag)::value>(au, av, na); });
-        CK(cudaEventRecord(ev[2], stream));
-        run_cache_service();
+        index_upkeep(na);
+        dispatch([&](auto tag) {
+            run_graphed(2, 0, na, [&] {
+                insert_phase_dev<decltype(tag)::value>(au, av, na);
+                rec(ev[2]);
+                run_cache_service();
+            });
+        });
         CK(cudaEventRecord(ev[3], stream));
         finish();
         fill_stats(s, 0, na, false, true);
+    }
+
+    // The launches of one traversal batch on the engine stream: whole-batch
+    // key sort, deletion phase, insertion phase, segment-table service.
+    // Queued directly or captured into a graph (run_graphed).
+    template <int A>
+    void batch_body(const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd, const uint32_t *d_au,
+                    const uint32_t *d_av, uint64_t na, cudaEvent_t mutation_after, cudaEvent_t e1, cudaEvent_t e2) {
+        presort_batch(d_du, d_dv, nd, d_au, d_av, na);
+        if (mutation_after) CK(cudaStreamWaitEvent(stream, mutation_after, 0));
+        delete_phase_dev<A>(d_du, d_dv, nd);
+        rec(e1);
+        insert_phase_dev<A>(d_au, d_av, na);
+        rec(e2);
+        presorted = false;
+        run_cache_service();
+    }
+
+    // One traversal batch through the graph cache.  Caller arrays are first
+    // copied into the engine's batch buffers, whose addresses the captured
+    // graphs hold.  `mutation_after` (a query wave's event) keeps the batch on
+    // direct launches.
+    void traversal_batch(const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd, const uint32_t *d_au,
+                         const uint32_t *d_av, uint64_t na, cudaEvent_t mutation_after, cudaEvent_t e1,
+                         cudaEvent_t e2) {
+        note_delete_phase(nd);
+        index_upkeep(na);
+        reserve_chunk_map(nd);
+        if (mutation_after || !use_graphs) {
+            dispatch([&](auto tag) {
+                batch_body<decltype(tag)::value>(d_du, d_dv, nd, d_au, d_av, na, mutation_after, e1, e2);
+            });
+            return;
+        }
+        const uint32_t *src[4] = {d_du, d_dv, d_au, d_av};
+        uint32_t *dst[4] = {du, dv, au, av};
+        const uint64_t cnt[4] = {nd, nd, na, na};
+        for (int a = 0; a < 4; ++a)
+            if (cnt[a] && src[a] != dst[a])
+                CK(cudaMemcpyAsync(dst[a], src[a], cnt[a] * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream));
+        dispatch([&](auto tag) {
+            run_graphed(0, nd, na, [&] {
+                batch_body<decltype(tag)::value>(du, dv, nd, au, av, na, nullptr, e1, e2);
+            });
+        });
     }
 
     // `mutation_after` (optional): an event the topology changes must wait
@@ -1648,19 +1873,10 @@ struct cig_handle {
                 pr_batch<float>(d_du, d_dv, nd, d_au, d_av, na);
             CK(cudaEventRecord(ev[1], stream));
             CK(cudaEventRecord(ev[2], stream));
+            run_cache_service();
         } else {
-            dispatch([&](auto tag) {
-                constexpr int A = decltype(tag)::value;
-                presort_batch(d_du, d_dv, nd, d_au, d_av, na);
-                if (mutation_after) CK(cudaStreamWaitEvent(stream, mutation_after, 0));
-                delete_phase_dev<A>(d_du, d_dv, nd);
-                CK(cudaEventRecord(ev[1], stream));
-                insert_phase_dev<A>(d_au, d_av, na);
-                CK(cudaEventRecord(ev[2], stream));
-                presorted = false;
-            });
+            traversal_batch(d_du, d_dv, nd, d_au, d_av, na, mutation_after, ev[1], ev[2]);
         }
-        run_cache_service();
         CK(cudaEventRecord(ev[3], stream));
         finish();
         fill_stats(s, nd, na, true, true);
@@ -1733,18 +1949,11 @@ struct cig_handle {
                     pr_batch<float>(b[i].del_u, b[i].del_v, b[i].nd, b[i].add_u, b[i].add_v, b[i].na);
                 CK(cudaEventRecord(e[1], stream));
                 CK(cudaEventRecord(e[2], stream));
+                run_cache_service();
             } else {
-                dispatch([&](auto tag) {
-                    constexpr int A = decltype(tag)::value;
-                    presort_batch(b[i].del_u, b[i].del_v, b[i].nd, b[i].add_u, b[i].add_v, b[i].na);
-                    delete_phase_dev<A>(b[i].del_u, b[i].del_v, b[i].nd);
-                    CK(cudaEventRecord(e[1], stream));
-                    insert_phase_dev<A>(b[i].add_u, b[i].add_v, b[i].na);
-                    CK(cudaEventRecord(e[2], stream));
-                    presorted = false;
-                });
+                traversal_batch(b[i].del_u, b[i].del_v, b[i].nd, b[i].add_u, b[i].add_v, b[i].na, nullptr, e[1],
+                                e[2]);
             }
-            run_cache_service();
             CK(cudaEventRecord(e[3], stream));
             if (digests) {
                 CK(cudaMemsetAsync(bdig + i, 0, sizeof(unsigned long long), stream));
@@ -2305,6 +2514,55 @@ struct cig_handle {
         }
     }
 
+    // Device bytes held, by part (cig_memory_info_get), from the sizes the
+    // allocations were made with.
+    void memory_info(cig_memory_info *m) const {
+        std::memset(m, 0, sizeof(*m));
+        const uint64_t nn = n, segs = fwd.seg_total, w = (nn + 31) / 32;
+        m->edge_cache = fwd.dev ? cache_slots * kSegEdges * sizeof(uint32_t) : 0;
+        m->segment_table = segs * (sizeof(int32_t) + 1 + sizeof(uint32_t)) +
+                           (refresh ? cache_slots * 2 * sizeof(uint32_t) + segs * sizeof(uint32_t) +
+                                          (kMaxEvict + kMaxAdmit + kCtlCount) * sizeof(uint32_t)
+                                    : 0);
+        m->descriptors = fwd.desc ? nn * sizeof(RowDesc) + sizeof(ArenaAlloc) : 0;
+        m->reverse_arena = rev.dev ? rev.seg_total * kSegEdges * sizeof(uint32_t) + nn * sizeof(RowDesc) +
+                                         sizeof(ArenaAlloc)
+                                   : 0;
+        for (const auto &b : ixb)
+            if (b.cap) m->position_index += b.cap * (sizeof(unsigned long long) + sizeof(uint2)) + w * sizeof(uint32_t);
+        uint64_t vs = 0;
+        if (loaded) {
+            vs += 2 * (nn + 1) * sizeof(uint32_t) + nn * sizeof(uint32_t);  // q0, q1, tmp_u32
+            if (inval_done) vs += (nn + 1) * sizeof(uint32_t);
+            if (opt.algo == CIG_PR) {
+                const uint64_t es = pr64 ? sizeof(double) : sizeof(float);
+                vs += 2 * nn * es + (nn + 1) * es + 2 * nn * sizeof(uint32_t);
+                if (!pr64) vs += nn * sizeof(float) + nn * sizeof(double) + 2 * w * sizeof(uint32_t) +
+                                 std::max<uint32_t>(pr_hubs, 1) * sizeof(double);
+            } else {
+                vs += nn * sizeof(unsigned long long) + 2 * nn * sizeof(uint32_t) + (nn + 1) * sizeof(uint32_t);
+            }
+        }
+        vs += sizeof(Status) + kSmallCount * sizeof(uint32_t) + 68 * sizeof(unsigned long long) +
+              kBigRowCap * sizeof(BigRow) + sizeof(TagState);
+        m->vertex_state = vs;
+        // Per slot of ensure_batch: 4 update arrays (4 B), 6 key/plan arrays
+        // (8 B), 12 group/match/chunk arrays (4 B), `touched` (2 x 4 B), the
+        // group type (1 B), flags + positions (2 x 4 x 4 B), group ends (2 x
+        // 4 B), packed whole-batch keys (2 x 4 x 8 B), addition groups (4 x 4 B).
+        const uint64_t per_slot = 16 + 48 + 48 + 8 + 1 + 32 + 8 + 64 + 16;
+        m->batch_buffers = bcap * per_slot + cub_bytes + chunk_map_cap * sizeof(uint32_t) +
+                           (opt.algo == CIG_PR ? 2 * bcap * sizeof(double) : 0) +
+                           static_cast<uint64_t>(bsnap_cap) * 41 * sizeof(unsigned long long);
+        if (qstream)
+            m->query_buffers = nn * kMsWidth * sizeof(uint32_t) + 3 * nn * sizeof(unsigned long long) +
+                               2 * (nn + 1) * sizeof(uint32_t) + sizeof(Status) + (8 + kMsWidth) * sizeof(uint32_t) +
+                               kBigRowCap * sizeof(BigRow);
+        m->total = m->edge_cache + m->segment_table + m->descriptors + m->reverse_arena + m->position_index +
+                   m->vertex_state + m->batch_buffers + m->query_buffers;
+        m->pinned_host = segs * kSegEdges * sizeof(uint32_t) + 4 * bcap * sizeof(uint32_t);
+    }
+
     // Make the pinned host arena current (write back dirty cache segments).
     void flush_host() {
         if (!loaded) throw CigError(CIG_ERR_ARG, "load a graph first");
@@ -2378,6 +2636,7 @@ int cig_options_default(cig_options *o) {
     o->max_batch = 0;
     o->arena_headroom_pct = 0;
     o->flags = 0;
+    o->index_budget_gib = 0.0;
     return CIG_OK;
 }
 
@@ -2568,6 +2827,13 @@ int cig_graph_info_get(cig_handle *h, cig_graph_info *info) {
         cudaMemGetInfo(&free_b, &total_b);
         info->device_bytes = total_b - free_b;
         info->pinned_bytes = h->fwd.seg_total * kSegEdges * sizeof(uint32_t);
+    });
+}
+
+int cig_memory_info_get(cig_handle *h, cig_memory_info *out) {
+    return guarded(h, [&] {
+        if (!out) throw CigError(CIG_ERR_ARG, "null output");
+        h->memory_info(out);
     });
 }
 

@@ -1,23 +1,27 @@
 // noalloc.cu - BFS depths over a device CSR without any allocation.
 //
-// Some callers cannot allocate device memory at the point where they need a
-// traversal: code running while a stream is being captured into a CUDA graph
-// (cudaMalloc is not capturable), latency-critical serving loops that must
-// not take cudaMalloc/cudaFree's implicit device synchronisation, and hosts
-// (plugins, embedded runtimes) whose memory pool is owned by someone else.
-// cig_bfs_csr_noalloc serves them: the caller passes the graph (device CSR)
-// and the output array; every piece of scratch (frontier queues, per-round
-// de-duplication stamps, counters, the grid barrier and the error word)
-// lives in one file-scope __device__ array of fixed size, so the call
-// performs no cudaMalloc, cudaFree or allocating library call.
+// Some callers cannot call cudaMalloc where they need a traversal: a plugin
+// or embedded runtime whose device memory belongs to a host framework with
+// its own pooling allocator (a raw cudaMalloc there bypasses the pool's
+// accounting and fails once the pool holds the memory), or a latency-bound
+// loop that must not take the device-wide synchronisation that cudaFree
+// implies.  cig_bfs_csr_noalloc serves them: the caller passes the graph
+// (device CSR) and the output array; every piece of scratch (frontier
+// queues, per-round de-duplication stamps, counters, the grid barrier and the
+// error word) lives in one file-scope __device__ array of fixed size, so the
+// call performs no cudaMalloc, cudaFree or allocating library call.  The call
+// is blocking: it reads the device error word back and synchronises the
+// caller's stream before it returns.
 //
 // Limits and sharing: at most kNoAllocMaxVertices vertices (about 3 MiB of
 // scratch, held by every GPU that loads the library until the process
-// exits).  All calls on a device share the same array and see what the last
-// call left in it; this file clears everything that must start at zero at the
-// start of each call.  Two calls whose work overlaps on one GPU (for example
-// on two streams) race on the shared array and must be serialised by the
-// caller.
+// exits); larger graphs are rejected with CIG_ERR_ARG.  The first call on a
+// device looks up the array's device address with that device current
+// (set-up), so it should come before any stream capture.  All calls on a
+// device share the same array and see what the last call left in it; each
+// call clears everything that must start at zero before its kernels read it.
+// Two calls whose work overlaps on one GPU (two host threads, or two streams)
+// race on the shared array and must be serialised by the caller.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -133,7 +137,8 @@ extern "C" int cig_bfs_csr_noalloc(const uint64_t *xadj, const uint32_t *adj, ui
                                    uint32_t *depth, void *stream_handle) {
     if (n == 0 || n > kNoAllocMaxVertices)
         return fail(CIG_ERR_ARG, "vertex count must be in [1, " + std::to_string(kNoAllocMaxVertices) + "]");
-    if (!xadj || !depth || source >= n) return fail(CIG_ERR_ARG, "null CSR/output pointer or source out of range");
+    if (!xadj || !adj || !depth || source >= n)
+        return fail(CIG_ERR_ARG, "null CSR/output pointer or source out of range");
     const cudaStream_t stream = static_cast<cudaStream_t>(stream_handle);
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);

@@ -315,195 +315,6 @@ __global__ void __launch_bounds__(kTpb) push_closure(AdjView fwd, unsigned long 
     }
 }
 
-// ---------------------------------------------------------------- asynchronous push closure
-// For the small frontiers of incremental batches the level-synchronous
-// closure spends most of its time at grid barriers (ncu, s22 batch: ~135
-// barrier stalls per issued instruction).  This variant has no rounds:
-// warps claim up to 32 queued vertices from a ring, relax their rows and
-// queue improved vertices again.  A vertex is in the ring at most once
-// (qstamp == T marks it queued); a row of kAsyncChunk entries or more is cut
-// into chunk items that other warps pick up, so the ring holds at most
-// n + m / kAsyncChunk items.  Label-correcting relaxation needs no order, so
-// the fixpoint (values and smallest-id parents) is the same.  The closure
-// ends when every reserved item has been processed (done == tail); every
-// wait is bounded.
-constexpr uint32_t kAsyncChunk = 1024;
-
-struct AsyncRing {
-    unsigned long long *slot;   // (vertex + 1) | chunk << 32; 0 = empty
-    unsigned long long *ctr;    // tail (reserved) at [kRingTail], head (claimed), done (processed):
-    uint32_t cap;               // each on its own 128-byte line
-};
-constexpr int kRingTail = 0, kRingHead = 16, kRingDone = 32, kRingCtrWords = 48;
-
-constexpr long long kAsyncWaitCycles = 4000000000LL;  // ~2 s at the B200's clock
-
-__device__ __forceinline__ unsigned long long ld_volatile64(const unsigned long long *p) {
-    return *reinterpret_cast<const volatile unsigned long long *>(p);
-}
-
-// Warp-aggregated append of `item` (lanes with want) to the ring.  All lanes call.
-__device__ __forceinline__ void ring_push(bool want, unsigned long long item, const AsyncRing &q, Status *st) {
-    const uint32_t mask = __ballot_sync(kFull, want);
-    if (!mask) return;
-    const uint32_t lane = lane_id();
-    const uint32_t leader = __ffs(mask) - 1;
-    unsigned long long base = 0;
-    if (lane == leader) base = atomicAdd(q.ctr + kRingTail, static_cast<unsigned long long>(__popc(mask)));
-    base = __shfl_sync(kFull, base, leader);
-    if (want) {
-        const uint32_t s = static_cast<uint32_t>((base + __popc(mask & lanemask_lt())) % q.cap);
-        // The slot's previous item was claimed long ago; wait until its reader freed it.
-        const long long t0 = clock64();
-        while (ld_volatile64(q.slot + s) != 0ull) {
-            if (clock64() - t0 > kAsyncWaitCycles) {
-                set_error(st, kErrBarrier, s);
-                return;
-            }
-        }
-        atomicExch(q.slot + s, item + 1ull);
-    }
-}
-
-template <int A>
-struct PushOpAsync {
-    uint32_t ccs;
-    unsigned long long *state;
-    uint32_t *qstamp;
-    uint32_t mark;  // "queued"
-    AsyncRing q;
-    Status *st;
-
-    __device__ __forceinline__ bool edge(bool valid, uint32_t x, uint32_t dx, uint32_t y) const {
-        bool want = false, improved = false;
-        if (valid) {
-            const uint32_t nd = relax_value<A>(dx, x, y, ccs);
-            const unsigned long long cand = pack(nd, x);
-            if (cand < __ldcg(state + y)) {
-                const unsigned long long old = atomicMin(state + y, cand);
-                improved = nd < val_of(old);
-                if (improved) {
-                    __threadfence();  // the new value is visible before y can be claimed again
-                    want = atomicExch(qstamp + y, mark) != mark;
-                }
-            }
-        }
-        ring_push(want, static_cast<unsigned long long>(y), q, st);
-        return improved;
-    }
-};
-
-// Initial items: the seed queue (q0, count), marked queued and copied in.
-__global__ void async_seed(const uint32_t *q0, const uint32_t *count, uint32_t *qstamp, const TagState *tags,
-                           AsyncRing ring, Status *st) {
-    const uint32_t mark = tags->next_tag + 1u;
-    const uint32_t n = *count;
-    const uint32_t rounded = (n + 31u) & ~31u;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rounded; i += gridDim.x * blockDim.x) {
-        bool want = false;
-        uint32_t x = 0;
-        if (i < n) {
-            x = q0[i];
-            want = atomicExch(qstamp + x, mark) != mark;
-        }
-        ring_push(want, static_cast<unsigned long long>(x), ring, st);
-    }
-}
-
-__global__ void advance_tag(TagState *tags, uint32_t by) { tags->next_tag += by; }
-
-// Ring positions are dealt to the warps round-robin: lane l of warp w takes
-// position w + (32 i + l) * warps.  A warp waits only on its own slots (no
-// shared claim counter for idle warps to fight over) and polls the tail and
-// done counters, read-only, while its next position is not reserved yet.
-template <int A>
-__global__ void __launch_bounds__(kTpb, 4) push_async(AdjView fwd, unsigned long long *state, uint32_t *qstamp,
-                                                      const TagState *tags, AsyncRing q, uint32_t *seg_hot,
-                                                      Status *st) {
-    __shared__ ExpandSmem<kTpb> sm;
-    ExpandCounters cnt;
-    const uint32_t mark = tags->next_tag + 1u;
-    const uint32_t lane = lane_id();
-    const unsigned long long warps = (gridDim.x * blockDim.x) >> 5;
-    const unsigned long long wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const PushOpAsync<A> op{(A == kCc) ? st->cc_shift : 0u, state, qstamp, mark, q, st};
-    unsigned long long pos = wid + lane * warps;  // this lane's next ring position
-    long long idle_since = 0;
-    uint32_t backoff = 32;
-    for (;;) {
-        if (ld_volatile(&st->err) & kErrBarrier) break;
-        const unsigned long long tail = ld_volatile64(q.ctr + kRingTail);
-        const bool mine = pos < tail;  // an item is (or will shortly be) in my slot
-        const uint32_t k = __popc(__ballot_sync(kFull, mine));
-        if (k == 0) {
-            // Done when every reserved item has been processed (done read
-            // first: done <= tail at all times).
-            uint32_t fin = 0;
-            if (lane == 0) {
-                const unsigned long long d = ld_volatile64(q.ctr + kRingDone);
-                fin = d == ld_volatile64(q.ctr + kRingTail);
-            }
-            if (__shfl_sync(kFull, fin, 0)) break;
-            if (!idle_since) idle_since = clock64();
-            if (clock64() - idle_since > kAsyncWaitCycles) {
-                if (lane == 0) set_error(st, kErrBarrier, 2u);
-                break;
-            }
-            __nanosleep(backoff);
-            backoff = min(backoff * 2u, 1024u);
-            continue;
-        }
-        idle_since = 0;
-        backoff = 32;
-        bool has = mine;
-        uint32_t x = 0, dx = 0, deg = 0, chunk = 0, nchunks = 0;
-        uint64_t off = 0;
-        if (mine) {
-            const uint32_t s = static_cast<uint32_t>(pos % q.cap);
-            const long long t0 = clock64();
-            unsigned long long v;
-            while ((v = ld_volatile64(q.slot + s)) == 0ull) {
-                if (clock64() - t0 > kAsyncWaitCycles) {
-                    set_error(st, kErrBarrier, 3u);
-                    break;
-                }
-            }
-            has = v != 0ull;
-            if (has) {
-                atomicExch(q.slot + s, 0ull);
-                v -= 1ull;
-                x = static_cast<uint32_t>(v);
-                chunk = static_cast<uint32_t>(v >> 32);
-                if (chunk == 0) atomicExch(qstamp + x, mark - 1u);  // dequeued: a later improvement queues x again
-                __threadfence();
-                dx = val_of(__ldcg(state + x));
-                const RowDesc d = fwd.desc[x];
-                deg = d.len;
-                off = d.off;
-                has = dx != kInf && deg > 0;
-                if (has && chunk == 0 && seg_hot) atomicAdd(seg_hot + (off >> kSegShift), deg);
-                if (has && deg >= kAsyncChunk) {
-                    // Long row: this lane takes chunk `chunk`, the others go back to the ring.
-                    if (chunk == 0) nchunks = (deg + kAsyncChunk - 1) / kAsyncChunk;
-                    off += static_cast<uint64_t>(chunk) * kAsyncChunk;
-                    deg = min(kAsyncChunk, deg - chunk * kAsyncChunk);
-                }
-            }
-            pos += 32ull * warps;
-        }
-        // Chunk items 1..nchunks-1 of long rows first, so other warps start on them.
-        for (uint32_t c = 1;; ++c) {
-            const bool want = c < nchunks;
-            if (!__any_sync(kFull, want)) break;
-            ring_push(want, (static_cast<unsigned long long>(c) << 32) | x, q, st);
-        }
-        expand_rows_warp<kTpb>(fwd, has, x, dx, off, deg, op, sm, cnt);
-        __threadfence();
-        if (lane == 0) atomicAdd(q.ctr + kRingDone, static_cast<unsigned long long>(k));
-    }
-    flush_counters(st, cnt, kCntPush);
-}
-
 // Persistent invalidation closure over the affected list.  Round r processes
 // list[lo, hi) and appends at list[hi + ...] counted by cnt[(r+1)%3].
 // Replaces RunSyncPushDDB_del rounds (framework.cuh:2830-2853).
@@ -564,7 +375,7 @@ struct LocalInvalOp {
 
 template <int A>
 __global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long long *state, uint32_t *aff_stamp,
-                                                      uint32_t epoch, uint32_t *list, uint32_t *cnt3,
+                                                      const uint32_t *epoch_p, uint32_t *list, uint32_t *cnt3,
                                                       uint32_t cap, BigList big, uint32_t max_rounds,
                                                       uint32_t max_sweeps, uint32_t *done, uint32_t *done_cnt,
                                                       uint32_t *aff_total, uint32_t *seg_hot, Status *st) {
@@ -573,6 +384,7 @@ __global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long
     __shared__ uint32_t lq_n[2];
     ExpandCounters c;
     const uint32_t ccs = (A == kCc) ? st->cc_shift : 0u;
+    const uint32_t epoch = *epoch_p;
     uint32_t lo = 0, hi = ld_volatile(cnt3 + 0);
     uint32_t r = 0;
     for (;; ++r) {
@@ -685,9 +497,10 @@ __global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long
 // 371-411), evaluated on the values before the batch.
 template <int A>
 __global__ void seed_deletions(const uint32_t *du, const uint32_t *dv, uint32_t nd, uint32_t n,
-                               const unsigned long long *state, uint32_t *aff_stamp, uint32_t epoch,
+                               const unsigned long long *state, uint32_t *aff_stamp, const uint32_t *epoch_p,
                                uint32_t *list, uint32_t *count, uint32_t cap, Status *st) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t epoch = *epoch_p;
     bool want = false;
     uint32_t v = 0;
     if (i < nd) {
@@ -710,6 +523,14 @@ __global__ void seed_deletions(const uint32_t *du, const uint32_t *dv, uint32_t 
     if (__any_sync(kFull, i < nd)) warp_enqueue(want, v, list, count, cap, st);
 }
 
+// Start of a deletion phase: advance the batch epoch (the "invalidated in
+// this batch" marker of aff_stamp, kept on the device so that a captured
+// batch graph needs no new arguments) and clear `count` counters.
+__global__ void phase_begin(uint32_t *epoch, uint32_t *counters, uint32_t count) {
+    if (threadIdx.x == 0) *epoch += 1u;
+    if (threadIdx.x < count) counters[threadIdx.x] = 0u;
+}
+
 // value <- initial value for every invalidated vertex (reset_affected_values,
 // driver.cuh:418-433): unreached for BFS/SSSP, its own id for CC.
 template <int A>
@@ -724,12 +545,12 @@ __global__ void reset_affected(const uint32_t *list, const uint32_t *total, unsi
 
 template <int A>
 __global__ void __launch_bounds__(kTpb) pull_repair(AdjView rev, unsigned long long *state, const uint32_t *aff_stamp,
-                                                    uint32_t epoch, const uint32_t *list, const uint32_t *total,
-                                                    BigList big, Status *st) {
+                                                    const uint32_t *epoch_p, const uint32_t *list,
+                                                    const uint32_t *total, BigList big, Status *st) {
     __shared__ ExpandSmem<kTpb> sm;
     ExpandCounters c;
     const uint32_t n = *total;
-    PullOp<A> op{(A == kCc) ? st->cc_shift : 0u, state, aff_stamp, epoch};
+    PullOp<A> op{(A == kCc) ? st->cc_shift : 0u, state, aff_stamp, *epoch_p};
     const Defer df{big.rows, big.cnt, big.cap, big.split};
     for (uint32_t base = 0; base < n; base += gridDim.x * kTpb) {
         const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
@@ -751,9 +572,9 @@ __global__ void __launch_bounds__(kTpb) pull_repair(AdjView rev, unsigned long l
 // The in-rows that pull_repair deferred, expanded by the whole grid.
 template <int A>
 __global__ void __launch_bounds__(kTpb) pull_deferred(AdjView rev, unsigned long long *state, const uint32_t *aff_stamp,
-                                                      uint32_t epoch, BigList big, Status *st) {
+                                                      const uint32_t *epoch_p, BigList big, Status *st) {
     ExpandCounters c;
-    PullOp<A> op{(A == kCc) ? st->cc_shift : 0u, state, aff_stamp, epoch};
+    PullOp<A> op{(A == kCc) ? st->cc_shift : 0u, state, aff_stamp, *epoch_p};
     expand_deferred<kTpb>(rev, big.rows, min(*big.cnt, big.cap), op, c);
     flush_counters(st, c, kCntPull);
 }

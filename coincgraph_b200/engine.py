@@ -40,7 +40,17 @@ class Options(ctypes.Structure):
         ("max_batch", ctypes.c_uint32),
         ("arena_headroom_pct", ctypes.c_uint32),
         ("flags", ctypes.c_uint32),
+        ("index_budget_gib", ctypes.c_double),
     ]
+
+
+class MemoryInfo(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_uint64) for name in (
+        "total", "edge_cache", "segment_table", "descriptors", "reverse_arena", "position_index", "vertex_state",
+        "batch_buffers", "query_buffers", "pinned_host")]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 class BatchStats(ctypes.Structure):
@@ -214,6 +224,7 @@ SIGNATURES = [
     ("cig_profile_enable", _i32, [_vp, _i32]),
     ("cig_profile_read", _i32, [_vp, ctypes.POINTER(StageProfile), _u32]),
     ("cig_bfs_csr_noalloc", _i32, [_vp, _vp, _u32, _u32, _vp, _vp]),
+    ("cig_memory_info_get", _i32, [_vp, ctypes.POINTER(MemoryInfo)]),
     ("cig_apply_batches_device", _i32, [_vp, ctypes.POINTER(UpdateBatch), _u32, ctypes.POINTER(BatchStats), _vp]),
     ("cig_autotune", _i32, [_vp, ctypes.POINTER(TuneResult)]),
     ("cig_serve_start", _i32, [_vp, ctypes.POINTER(ServeOptions)]),
@@ -277,7 +288,7 @@ class Engine:
 
     def __init__(self, algo="sssp", device: int = 0, source: int = 0, cache_gib: float = 4.0,
                  cache_compat: bool = False, pr_epsilon: float = 1e-6, pr_max_rounds: int = 100,
-                 max_batch: int = 0, headroom_pct: int = 0, flags: int = 0):
+                 max_batch: int = 0, headroom_pct: int = 0, flags: int = 0, index_budget_gib: float = 0.0):
         self.lib = load_library()
         o = default_options()
         o.algo = ALGOS[algo] if isinstance(algo, str) else int(algo)
@@ -290,6 +301,7 @@ class Engine:
         o.max_batch = max_batch
         o.arena_headroom_pct = headroom_pct
         o.flags = flags
+        o.index_budget_gib = index_budget_gib
         self.options = o
         h = ctypes.c_void_p()
         rc = self.lib.cig_create(ctypes.byref(o), ctypes.byref(h))
@@ -510,6 +522,12 @@ class Engine:
         arr = (StageProfile * len(STAGES))()
         self._check(self.lib.cig_profile_read(self.h, arr, len(STAGES)))
         return {name: arr[i].as_dict() for i, name in enumerate(STAGES)}
+
+    def memory(self) -> dict:
+        """Device bytes held by this handle, by part (cig_memory_info_get)."""
+        m = MemoryInfo()
+        self._check(self.lib.cig_memory_info_get(self.h, ctypes.byref(m)))
+        return m.as_dict()
 
     def info(self) -> dict:
         g = GraphInfo()

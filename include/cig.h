@@ -56,6 +56,9 @@ typedef struct {
     uint32_t max_batch;      /* largest deletion or insertion phase to size buffers for (0: grow) */
     uint32_t arena_headroom_pct; /* extra arena capacity in percent (0: default 12.5%) */
     uint32_t flags;          /* CIG_FLAG_* */
+    double index_budget_gib; /* device bytes for the two position-index tables, GiB (0: a quarter of the
+                                free device memory per table); the indexed row-class threshold rises until
+                                the tables fit, and rows of smaller classes fall back to the row scan */
 } cig_options;
 
 #define CIG_FLAG_NO_CACHE_REFRESH 0x1u /* keep the segment residency chosen at load */
@@ -99,6 +102,24 @@ typedef struct {
     uint64_t device_bytes;
     uint64_t pinned_bytes;
 } cig_graph_info;
+
+/* Device memory held by a handle, by part (bytes).  No reference
+ * counterpart (the reference sizes its cache in graph_datum.cuh:158-176 and
+ * keeps its reverse index in host memory). */
+typedef struct {
+    uint64_t total;          /* sum of the parts below */
+    uint64_t edge_cache;     /* HBM edge cache (the --cache budget, whole 64 KiB segments) */
+    uint64_t segment_table;  /* segment -> cache-slot map, dirty flags, scores, free stack */
+    uint64_t descriptors;    /* forward row descriptors (16 B per vertex) */
+    uint64_t reverse_arena;  /* device-only in-edge arena and its descriptors */
+    uint64_t position_index; /* both position-index tables and row bitmaps */
+    uint64_t vertex_state;   /* values/parents, stamps, frontier queues, PR arrays */
+    uint64_t batch_buffers;  /* per-batch update, key, group and sort scratch buffers */
+    uint64_t query_buffers;  /* multi-source query buffers (allocated on first query) */
+    uint64_t pinned_host;    /* pinned mapped host arena + staging (host memory, not in total) */
+} cig_memory_info;
+
+int cig_memory_info_get(cig_handle *h, cig_memory_info *out);
 
 /* Fill `o` with the reference's defaults (app_skeleton.h:42-90 and the
  * per-sample flags). */
@@ -326,20 +347,25 @@ int cig_profile_read(cig_handle *h, cig_stage_profile *out, uint32_t count);
 
 /* BFS depths over a CSR already in device memory, with no device
  * allocation.  No counterpart in the reference.  For callers that cannot
- * allocate at the point of use: code running during CUDA stream capture
- * (cudaMalloc cannot be captured), serving loops that must avoid
- * cudaMalloc/cudaFree and their implicit device synchronisation, and hosts
- * whose device memory pool belongs to someone else.
- *   xadj[n+1] (uint64) and adj[xadj[n]] (uint32): device CSR, rows in any order;
+ * call cudaMalloc where they need a traversal: plugins and embedded runtimes
+ * whose device memory belongs to a host framework with its own allocator
+ * (raw cudaMalloc/cudaFree there bypass its accounting and can fail once the
+ * pool holds the memory), and latency-bound loops that must not take the
+ * device-wide synchronisation cudaFree implies.
+ *   xadj[n+1] (uint64) and adj[xadj[n]] (uint32): device CSR, rows in any
+ *   order; both must be non-null (an edge-free graph passes a dummy adj);
  *   depth[n] (uint32): device output, 0xFFFFFFFF for unreached vertices;
- *   stream: a cudaStream_t (NULL = the legacy default stream); the call
- *   returns after the work on that stream has finished.
+ *   stream: a cudaStream_t (NULL = the legacy default stream).  The call is
+ *   blocking: it copies the device error word to the host and synchronises
+ *   `stream` before it returns.
  * All scratch lives in a fixed __device__ array sized for at most
- * CIG_NOALLOC_MAX_VERTICES vertices (about 3 MiB held by every GPU that loads
- * the library); larger n is rejected with CIG_ERR_ARG.  The first call on a
- * device looks up that array's device address, so make the first call on
- * each device before any stream capture.  Calls on one device share the
- * array: calls that overlap on the GPU race and must be serialised.
+ * CIG_NOALLOC_MAX_VERTICES vertices (about 3 MiB, held by every GPU that
+ * loads the library until the process exits); larger n is rejected with
+ * CIG_ERR_ARG.  The first call on a device looks up that array's device
+ * address (set-up), so make the first call on each device before any stream
+ * capture.  Calls on one device share the array and each starts by clearing
+ * what must start at zero: calls that overlap on the GPU (two host threads,
+ * two streams) race and must be serialised by the caller.
  * Errors: the message is available from cig_last_error(NULL). */
 #define CIG_NOALLOC_MAX_VERTICES (1u << 18)
 int cig_bfs_csr_noalloc(const uint64_t *xadj, const uint32_t *adj, uint32_t n, uint32_t source, uint32_t *depth,

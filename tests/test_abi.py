@@ -55,7 +55,8 @@ def test_options_defaults_match_reference_flags(built):
 def test_struct_layouts(built):
     from coincgraph_b200 import engine
 
-    assert ctypes.sizeof(engine.Options) == 48
+    assert ctypes.sizeof(engine.Options) == 56
+    assert ctypes.sizeof(engine.MemoryInfo) == 10 * 8
     assert ctypes.sizeof(engine.BatchStats) == 20 * 8
     assert ctypes.sizeof(engine.StageProfile) == 6 * 8
     assert ctypes.sizeof(engine.QueryStats) == 8 * 8

@@ -372,13 +372,3 @@ def test_cc_saturated_depths(bits, monkeypatch):
     run_case(adversarial_case(), "cc", CACHES["resident"])
     run_case(grid_case(24, 3, 80), "cc", CACHES["resident"])
     run_case_whole_batches(rmat_case(10, 3, 200, 200, seed_offset=21, symmetric=True), "cc", CACHES["mixed"])
-
-
-@pytest.mark.parametrize("algo", ["bfs", "sssp", "cc"])
-def test_async_push_closure(algo, monkeypatch):
-    """The barrier-free push closure (CIG_ASYNC_PUSH=1, off by default) gives
-    the oracle's values, parent witnesses and rows on short closures."""
-    monkeypatch.setenv("CIG_ASYNC_PUSH", "1")
-    run_case(rmat_case(11, 3, 300, 300, seed_offset=22), algo, CACHES["resident"])
-    run_case(adversarial_case(), algo, CACHES["resident"])
-    run_case_whole_batches(big_row_case(), algo, CACHES["mixed"])
