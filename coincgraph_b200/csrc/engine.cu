@@ -700,16 +700,19 @@ struct cig_handle {
         BatchGraph &r = graphs.back();
         CK(cudaGraphLaunch(r.exec, stream));
         n_launch += r.launches;
+        ++graph_replays;
         r.last_use = ++graph_clock;
         if (prof_on) prof_pending.insert(prof_pending.end(), r.prof_recs.begin(), r.prof_recs.end());
     }
 
     uint64_t launch_mark = 0;
 
+    uint64_t replay_mark = 0;
     void reset_counters() {
         presorted = false;
         CK(cudaMemsetAsync(status->counters, 0, sizeof(status->counters), stream));
         launch_mark = n_launch;
+        replay_mark = graph_replays;
     }
 
     void require_alive() const {
@@ -1436,12 +1439,18 @@ struct cig_handle {
     // and reverse deletion keys), t1/t2 (addition keys) and their groups, and
     // sets `presorted` for the two phases that follow.  Returns false (and
     // leaves the per-phase sorts to the phases) when the fields do not fit.
-    bool presort_batch(const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd, const uint32_t *d_au,
-                       const uint32_t *d_av, uint64_t na) {
+    uint32_t presort_field_bits(uint64_t nd, uint64_t na) const {
         const uint64_t mx = std::max<uint64_t>(n, std::max(nd, na));
         uint32_t f = 0;
         while (f < 32 && (1ull << f) <= mx) ++f;
-        if (2 + 2 * f > 64) return false;
+        return f;
+    }
+    bool presort_fits(uint64_t nd, uint64_t na) const { return 2 + 2 * presort_field_bits(nd, na) <= 64; }
+
+    bool presort_batch(const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd, const uint32_t *d_au,
+                       const uint32_t *d_av, uint64_t na) {
+        const uint32_t f = presort_field_bits(nd, na);
+        if (!presort_fits(nd, na)) return false;
         PackedSets ps{};
         ps.off[0] = 0;
         ps.off[1] = static_cast<uint32_t>(nd);
@@ -1805,37 +1814,24 @@ struct cig_handle {
         stage_batch(nullptr, nullptr, 0, hu, hv, na);
         index_upkeep(na);
         dispatch([&](auto tag) {
-            run_graphed(2, 0, na, [&] {
-                insert_phase_dev<decltype(tag)::value>(au, av, na);
-                rec(ev[2]);
-                run_cache_service();
-            });
+            run_graphed(2, 0, na, [&] { insert_phase_dev<decltype(tag)::value>(au, av, na); });
         });
+        CK(cudaEventRecord(ev[2], stream));
+        cache_service_graphed();
         CK(cudaEventRecord(ev[3], stream));
         finish();
         fill_stats(s, 0, na, false, true);
     }
 
     // The launches of one traversal batch on the engine stream: whole-batch
-    // key sort, deletion phase, insertion phase, segment-table service.
-    // Queued directly or captured into a graph (run_graphed).
-    template <int A>
-    void batch_body(const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd, const uint32_t *d_au,
-                    const uint32_t *d_av, uint64_t na, cudaEvent_t mutation_after, cudaEvent_t e1, cudaEvent_t e2) {
-        presort_batch(d_du, d_dv, nd, d_au, d_av, na);
-        if (mutation_after) CK(cudaStreamWaitEvent(stream, mutation_after, 0));
-        delete_phase_dev<A>(d_du, d_dv, nd);
-        rec(e1);
-        insert_phase_dev<A>(d_au, d_av, na);
-        rec(e2);
-        presorted = false;
-        run_cache_service();
-    }
-
-    // One traversal batch through the graph cache.  Caller arrays are first
-    // copied into the engine's batch buffers, whose addresses the captured
-    // graphs hold.  `mutation_after` (a query wave's event) keeps the batch on
-    // direct launches.
+    // key sort and deletion phase, then insertion phase (on the presorted
+    // keys), then the segment-table service.  The three parts are queued
+    // directly or each replayed from a graph (run_graphed), with the phase
+    // events e1, e2 recorded between them on the stream, so per-phase device
+    // times stay exact for every batch.  Caller arrays are first copied into
+    // the engine's batch buffers, whose addresses the graphs hold.
+    // `mutation_after` (a query wave's event) keeps the batch on direct
+    // launches.
     void traversal_batch(const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd, const uint32_t *d_au,
                          const uint32_t *d_av, uint64_t na, cudaEvent_t mutation_after, cudaEvent_t e1,
                          cudaEvent_t e2) {
@@ -1844,8 +1840,16 @@ struct cig_handle {
         reserve_chunk_map(nd);
         if (mutation_after || !use_graphs) {
             dispatch([&](auto tag) {
-                batch_body<decltype(tag)::value>(d_du, d_dv, nd, d_au, d_av, na, mutation_after, e1, e2);
+                constexpr int A = decltype(tag)::value;
+                presort_batch(d_du, d_dv, nd, d_au, d_av, na);
+                if (mutation_after) CK(cudaStreamWaitEvent(stream, mutation_after, 0));
+                delete_phase_dev<A>(d_du, d_dv, nd);
+                CK(cudaEventRecord(e1, stream));
+                insert_phase_dev<A>(d_au, d_av, na);
+                CK(cudaEventRecord(e2, stream));
+                presorted = false;
             });
+            run_cache_service();
             return;
         }
         const uint32_t *src[4] = {d_du, d_dv, d_au, d_av};
@@ -1855,10 +1859,28 @@ struct cig_handle {
             if (cnt[a] && src[a] != dst[a])
                 CK(cudaMemcpyAsync(dst[a], src[a], cnt[a] * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream));
         dispatch([&](auto tag) {
-            run_graphed(0, nd, na, [&] {
-                batch_body<decltype(tag)::value>(du, dv, nd, au, av, na, nullptr, e1, e2);
+            constexpr int A = decltype(tag)::value;
+            bool sorted = false;
+            run_graphed(3, nd, na, [&] {
+                sorted = presort_batch(du, dv, nd, au, av, na);
+                delete_phase_dev<A>(du, dv, nd);
             });
+            // A replay runs no host code: the whole-batch sort's outcome is
+            // a function of the shape.
+            presorted = sorted || presort_fits(nd, na);
+            CK(cudaEventRecord(e1, stream));
+            run_graphed(4, nd, na, [&] { insert_phase_dev<A>(au, av, na); });
+            presorted = false;
+            CK(cudaEventRecord(e2, stream));
         });
+        cache_service_graphed();
+    }
+
+    void cache_service_graphed() {
+        if (refresh)
+            run_graphed(5, 0, 0, [&] { run_cache_service(); });
+        else
+            run_cache_service();
     }
 
     // `mutation_after` (optional): an event the topology changes must wait
@@ -1936,9 +1958,19 @@ struct cig_handle {
             CK(cudaEventCreate(&e));
             bev.push_back(e);
         }
-        std::vector<uint64_t> launches(count);
+        // The stage profiler resolves once per call: keep a profiled batched
+        // call on direct launches (a graph replayed twice in one call would
+        // leave only its last replay's event times).
+        const bool graphs_saved = use_graphs;
+        if (prof_on) use_graphs = false;
+        struct Restore {
+            bool &flag;
+            bool value;
+            ~Restore() { flag = value; }
+        } restore{use_graphs, graphs_saved};
+        std::vector<uint64_t> launches(count), replays(count);
         for (uint32_t i = 0; i < count; ++i) {
-            const uint64_t l0 = n_launch;
+            const uint64_t l0 = n_launch, r0 = graph_replays;
             reset_counters();
             cudaEvent_t *e = bev.data() + 4ull * i;
             CK(cudaEventRecord(e[0], stream));
@@ -1963,6 +1995,7 @@ struct cig_handle {
                                cudaMemcpyDeviceToDevice, stream));
             check_launch();
             launches[i] = n_launch - l0;
+            replays[i] = graph_replays - r0;
         }
         finish();
         std::vector<unsigned long long> snap(40ull * count);
@@ -1972,13 +2005,16 @@ struct cig_handle {
             CK(cudaMemcpy(digests, bdig, count * sizeof(uint64_t), cudaMemcpyDeviceToHost));
         }
         for (uint32_t i = 0; i < count; ++i)
-            if (stats)
+            if (stats) {
                 fill_stats_from(stats + i, snap.data() + 40ull * i, bev.data() + 4ull * i, launches[i], b[i].nd,
                                 b[i].na, true, true);
+                stats[i].graph_replays = replays[i];
+            }
     }
 
     void fill_stats(cig_batch_stats *s, uint64_t nd, uint64_t na, bool del, bool ins) {
         fill_stats_from(s, h_status->counters, ev, n_launch - launch_mark, nd, na, del, ins);
+        if (s) s->graph_replays = graph_replays - replay_mark;
     }
 
     void fill_stats_from(cig_batch_stats *s, const unsigned long long *c, const cudaEvent_t *evs, uint64_t launches,
@@ -2001,16 +2037,18 @@ struct cig_handle {
         s->cache_segments_evicted = c[kCntSegEvicted];
         s->pr_rounds = c[kCntPrRounds];
         s->kernel_launches = launches;
-        float ms = 0;
-        if (del) {
-            cudaEventElapsedTime(&ms, evs[0], evs[1]);
-            s->ms_delete = ms;
-        }
+        auto elapsed = [](cudaEvent_t a, cudaEvent_t b) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+                cudaGetLastError();  // leave no error behind for the next call
+                return -1.0;
+            }
+            return static_cast<double>(ms);
+        };
+        if (del) s->ms_delete = elapsed(evs[0], evs[1]);
         if (ins) {
-            cudaEventElapsedTime(&ms, evs[1], evs[2]);
-            s->ms_insert = ms;
-            cudaEventElapsedTime(&ms, evs[2], evs[3]);
-            s->ms_cache = ms;
+            s->ms_insert = elapsed(evs[1], evs[2]);
+            s->ms_cache = elapsed(evs[2], evs[3]);
         }
         if (opt.algo == CIG_PR) {
             double l1 = 0;

@@ -72,6 +72,39 @@ struct Defer {
     uint32_t split;   // rows of at least this many entries are deferred
 };
 
+// Sweep of one row by `lanes` threads (a warp or a block; `t` = the
+// thread's rank among them).  Rows start on a 16-byte boundary in the
+// arenas (a block of 2^c >= 4 slots is aligned to its size), so each thread
+// reads four consecutive entries with one 16-byte load: a warp moves 128
+// entries, 512 bytes, per step, and a zero-copy row crosses the host link
+// in full 16-byte requests.  Entries past `deg` (still inside the block,
+// whose size is a multiple of 4) are masked.  A row that is not 16-byte
+// aligned (a caller's plain CSR) is read one entry per thread.  Every
+// thread of the group runs the same number of steps (Op::edge is
+// warp-synchronous).
+template <uint32_t lanes, class Op, class P>
+__device__ __forceinline__ void sweep_row(const uint32_t *rp, uint32_t deg, uint32_t t, uint32_t x, P payload,
+                                          const Op &op, ExpandCounters &cnt) {
+    if ((reinterpret_cast<uintptr_t>(rp) & 15u) == 0) {
+        for (uint32_t base = 0; base < deg; base += 4u * lanes) {
+            const uint32_t k = base + 4u * t;
+            uint4 q = make_uint4(kTomb, kTomb, kTomb, kTomb);
+            if (k < deg) q = __ldg(reinterpret_cast<const uint4 *>(rp + k));
+            cnt.hits += op.edge(k < deg && q.x != kTomb, x, payload, q.x);
+            cnt.hits += op.edge(k + 1u < deg && q.y != kTomb, x, payload, q.y);
+            cnt.hits += op.edge(k + 2u < deg && q.z != kTomb, x, payload, q.z);
+            cnt.hits += op.edge(k + 3u < deg && q.w != kTomb, x, payload, q.w);
+        }
+    } else {
+        for (uint32_t base = 0; base < deg; base += lanes) {
+            const uint32_t k = base + t;
+            const bool valid = k < deg;
+            const uint32_t y = valid ? __ldg(rp + k) : 0u;
+            cnt.hits += op.edge(valid && y != kTomb, x, payload, y);
+        }
+    }
+}
+
 // Op must provide: __device__ bool edge(bool valid, uint32_t x, P payload, uint32_t y) const;
 // returning true when the edge changed state.
 // edge() is called by all 32 lanes of a warp together (valid=false on padding lanes).
@@ -112,13 +145,7 @@ __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint3
         const P bp = sm.b_payload;
         const uint64_t boff = sm.b_off;
         if (bdeg <= kSegEdges) {
-            const uint32_t *rp = view.at(boff);
-            for (uint32_t base = 0; base < bdeg; base += TPB) {
-                const uint32_t k = base + threadIdx.x;
-                const bool valid = k < bdeg;
-                const uint32_t y = valid ? __ldg(rp + k) : 0u;
-                cnt.hits += op.edge(valid && y != kTomb, bx, bp, y);
-            }
+            sweep_row<TPB>(view.at(boff), bdeg, threadIdx.x, bx, bp, op, cnt);
         } else {
             for (uint32_t base = 0; base < bdeg; base += TPB) {
                 const uint32_t k = base + threadIdx.x;
@@ -140,13 +167,7 @@ __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint3
         const uint32_t wdeg = __shfl_sync(kFull, deg, leader);
         const uint64_t woff = __shfl_sync(kFull, static_cast<unsigned long long>(off), leader);
         if (lane == leader) med = false;
-        const uint32_t *rp = view.at(woff);
-        for (uint32_t base = 0; base < wdeg; base += 32u) {
-            const uint32_t k = base + lane;
-            const bool valid = k < wdeg;
-            const uint32_t y = valid ? __ldg(rp + k) : 0u;
-            cnt.hits += op.edge(valid && y != kTomb, wx, wp, y);
-        }
+        sweep_row<32u>(view.at(woff), wdeg, lane, wx, wp, op, cnt);
     }
 
     // Tier 3: small rows gathered through a warp scan.
@@ -202,109 +223,14 @@ __device__ __forceinline__ void expand_deferred(const AdjView &view, const BigRo
         const uint64_t chunks = (r.deg + kSplitChunk - 1) / kSplitChunk;
         uint64_t g = prefix + (blockIdx.x + grid - static_cast<uint32_t>(prefix % grid)) % grid;
         for (; g < prefix + chunks; g += grid) {
+            // A chunk (1024 entries, a multiple of 4) never straddles a
+            // segment boundary: one pointer serves it.
             const uint32_t base = static_cast<uint32_t>(g - prefix) * kSplitChunk;
-            for (uint32_t kk = 0; kk < kSplitChunk; kk += TPB) {
-                const uint32_t k = base + kk + threadIdx.x;
-                const bool valid = k < r.deg;
-                const uint32_t y = valid ? __ldg(view.at(r.off + k)) : 0u;
-                cnt.hits += op.edge(valid && y != kTomb, r.x, static_cast<P>(r.payload), y);
-            }
+            const uint32_t len = min(kSplitChunk, r.deg - base);
+            sweep_row<TPB>(view.at(r.off + base), len, threadIdx.x, r.x, static_cast<P>(r.payload), op, cnt);
         }
         prefix += chunks;
     }
-}
-
-}  // namespace cig
-
-namespace cig {
-
-// Warp-only expansion (no block-wide tier and no __syncthreads, so the warps
-// of a block run independently): rows of 32 or more entries are swept by the
-// whole warp one at a time, shorter rows are gathered as in tier 3 of
-// expand_rows; rows of at least `defer.split` entries go to the deferred
-// list as in expand_rows.  `sm` slots [warp*32, warp*32+32) belong to the
-// calling warp.  All 32 lanes must call.
-template <int TPB, class Op, class P>
-__device__ __forceinline__ void expand_rows_warp(const AdjView &view, bool has, uint32_t x, P payload, uint64_t off,
-                                                 uint32_t deg, const Op &op, ExpandSmem<TPB, P> &sm,
-                                                 ExpandCounters &cnt, const Defer &defer = Defer{nullptr, nullptr, 0, 0}) {
-    const uint32_t lane = lane_id();
-    const uint32_t warp = threadIdx.x >> 5;
-    if (has) {
-        cnt.rows += 1;
-        cnt.edges += deg;
-        if (view.cached(off)) cnt.edges_cached += deg;
-    }
-    if (has && defer.rows && deg >= defer.split) {
-        const uint32_t i = atomicAdd(defer.count, 1u);
-        if (i < defer.cap) {
-            defer.rows[i] = BigRow{off, static_cast<unsigned long long>(payload), x, deg};
-            has = false;
-        }
-    }
-    bool med = has && deg >= 32u;
-    uint32_t mmask;
-    while ((mmask = __ballot_sync(kFull, med)) != 0u) {
-        const uint32_t leader = __ffs(mmask) - 1;
-        const uint32_t wx = __shfl_sync(kFull, x, leader);
-        const P wp = __shfl_sync(kFull, payload, leader);
-        const uint32_t wdeg = __shfl_sync(kFull, deg, leader);
-        const uint64_t woff = __shfl_sync(kFull, static_cast<unsigned long long>(off), leader);
-        if (lane == leader) med = false;
-        if (wdeg <= kSegEdges) {
-            const uint32_t *rp = view.at(woff);  // a block of <= 2^14 slots lies in one segment
-            for (uint32_t base = 0; base < wdeg; base += 32u) {
-                const uint32_t k = base + lane;
-                const bool valid = k < wdeg;
-                const uint32_t y = valid ? __ldg(rp + k) : 0u;
-                cnt.hits += op.edge(valid && y != kTomb, wx, wp, y);
-            }
-        } else {
-            for (uint32_t base = 0; base < wdeg; base += 32u) {
-                const uint32_t k = base + lane;
-                const bool valid = k < wdeg;
-                const uint32_t y = valid ? __ldg(view.at(woff + k)) : 0u;
-                cnt.hits += op.edge(valid && y != kTomb, wx, wp, y);
-            }
-        }
-    }
-    const uint32_t mydeg = (has && deg < 32u) ? deg : 0u;
-    uint32_t incl = mydeg;
-#pragma unroll
-    for (uint32_t o = 1; o < 32u; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(kFull, incl, o);
-        if (lane >= o) incl += t;
-    }
-    const uint32_t total = __shfl_sync(kFull, incl, 31);
-    if (total == 0) return;
-    const uint32_t wb = warp * 32u;
-    __syncwarp();
-    sm.f_scan[wb + lane] = incl - mydeg;
-    sm.f_x[wb + lane] = x;
-    sm.f_payload[wb + lane] = payload;
-    sm.f_ptr[wb + lane] = mydeg ? view.at(off) : nullptr;
-    __syncwarp();
-    for (uint32_t base = 0; base < total; base += 32u) {
-        const uint32_t e = base + lane;
-        const bool valid = e < total;
-        uint32_t ox = 0, y = 0;
-        P op_ = 0;
-        if (valid) {
-            uint32_t lo = 0, hi = 32;
-            while (hi - lo > 1) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (sm.f_scan[wb + mid] <= e)
-                    lo = mid;
-                else
-                    hi = mid;
-            }
-            ox = sm.f_x[wb + lo];
-            op_ = sm.f_payload[wb + lo];
-            y = __ldg(sm.f_ptr[wb + lo] + (e - sm.f_scan[wb + lo]));
-        }
-        cnt.hits += op.edge(valid && y != kTomb, ox, op_, y);
-    }
-    __syncwarp();
 }
 
 }  // namespace cig

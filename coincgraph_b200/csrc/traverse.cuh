@@ -207,7 +207,7 @@ struct LocalPushOp {
 };
 
 template <int A>
-__global__ void __launch_bounds__(kTpb) push_closure(AdjView fwd, unsigned long long *state, uint32_t *qstamp,
+__global__ void __launch_bounds__(kTpb, 4) push_closure(AdjView fwd, unsigned long long *state, uint32_t *qstamp,
                                                      TagState *tags, Frontier fr, BigList big, uint32_t max_rounds,
                                                      uint32_t max_sweeps, uint32_t *seg_hot, Status *st) {
     __shared__ ExpandSmem<kTpb> sm;
@@ -374,7 +374,7 @@ struct LocalInvalOp {
 };
 
 template <int A>
-__global__ void __launch_bounds__(kTpb) inval_closure(AdjView fwd, unsigned long long *state, uint32_t *aff_stamp,
+__global__ void __launch_bounds__(kTpb, 4) inval_closure(AdjView fwd, unsigned long long *state, uint32_t *aff_stamp,
                                                       const uint32_t *epoch_p, uint32_t *list, uint32_t *cnt3,
                                                       uint32_t cap, BigList big, uint32_t max_rounds,
                                                       uint32_t max_sweeps, uint32_t *done, uint32_t *done_cnt,

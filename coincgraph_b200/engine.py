@@ -75,6 +75,7 @@ class BatchStats(ctypes.Structure):
         ("pr_rounds", ctypes.c_uint64),
         ("pr_residual_l1", ctypes.c_double),
         ("kernel_launches", ctypes.c_uint64),
+        ("graph_replays", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:

@@ -87,7 +87,9 @@ typedef struct {
     double ms_cache;             /* device time of cache maintenance */
     uint64_t pr_rounds;
     double pr_residual_l1;       /* FP64 L1 norm of the PR residual after the batch */
-    uint64_t kernel_launches;    /* engine kernels launched by the call (library sort kernels excluded) */
+    uint64_t kernel_launches;    /* engine kernels launched by the call (library sort kernels excluded),
+                                    directly or as nodes of a replayed graph */
+    uint64_t graph_replays;      /* captured batch graphs launched by the call (0: direct launches) */
 } cig_batch_stats;
 
 typedef struct {

@@ -57,7 +57,7 @@ def test_struct_layouts(built):
 
     assert ctypes.sizeof(engine.Options) == 56
     assert ctypes.sizeof(engine.MemoryInfo) == 10 * 8
-    assert ctypes.sizeof(engine.BatchStats) == 20 * 8
+    assert ctypes.sizeof(engine.BatchStats) == 21 * 8
     assert ctypes.sizeof(engine.StageProfile) == 6 * 8
     assert ctypes.sizeof(engine.QueryStats) == 8 * 8
     assert ctypes.sizeof(engine.UpdateBatch) == 6 * 8
