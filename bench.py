@@ -55,6 +55,12 @@ def parse_args():
     p.add_argument("--algo", default="sssp", choices=["bfs", "sssp", "cc"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-parity", action="store_true", help="skip the oracle replay after the timed region")
+    p.add_argument("--no-extras", action="store_true",
+                   help="stream: skip the uneven batched-vs-plain and served measurements after the main line")
+    p.add_argument("--index-budget", type=float, default=0.0,
+                   help="GiB for the two position-index tables (0: a quarter of free device memory each)")
+    p.add_argument("--served-requests", type=int, default=200, help="default line: served-stream requests")
+    p.add_argument("--served-rate", type=float, default=40.0, help="default line: served Poisson rate, requests/s")
     p.add_argument("--ref-budget-s", type=float, default=150.0,
                    help="reference arm: stop timing after this much CPU time")
     p.add_argument("--workload", default="stream",
@@ -204,39 +210,81 @@ ROW_BYTES, EDGE_STATE_BYTES, ADJ_BYTES, HIT_BYTES = 28, 8, 4, 16
 # its segment is resident, else the host link); per deletion key an 8-byte
 # key read and a 4-byte first-match word.
 DEL_KEY_BYTES = 12
+# Whole-batch key sort, per key (4 keys per update pair): 8 B written by
+# make_keys_batch, 7 radix passes of 8 B read + 8 B written, 20 B by
+# unpack_keys_batch (key read, key + flag written), 8 B by the flag scan and
+# 16 B by group_scatter_batch.
+SORT_KEY_BYTES = 8 + 7 * 16 + 20 + 8 + 16
+# Deletion phase per request and arena (mutate, mutate_rev; the row scan is
+# billed to del_scan): key 8 B + descriptor 16 B (del_classify), index probe
+# 16 B read + 8 B written (del_index), tombstone 4 B + first match 4 B
+# (del_apply), descriptor 16 B written (del_finish).
+DEL_REQ_BYTES = 8 + 16 + 24 + 8 + 16
+# Addition phase per request and arena (add, add_rev): key 8 B + plan 8 B +
+# descriptor 16 B read and 16 B written + value 4 B + index entry 16 B; per
+# entry of a relocated row 4 B read + 4 B written.
+ADD_REQ_BYTES = 8 + 8 + 32 + 4 + 16
+MOVE_ENTRY_BYTES = 8
+# Segment-table service: a loaded or evicted 64 KiB segment crosses the host
+# link once and is read or written once in HBM.
+SEG_BYTES = 65536
+
+# Kernels of each profiler stage (the stage time covers all of them).
+STAGE_KERNELS = {
+    "group": "make_keys_batch + CUB radix sort + unpack_keys_batch + scan + group_scatter_batch",
+    "mutate": "del_classify, del_chunk_map, del_scan, del_index, del_apply, del_finish, mutate_delete(_big), "
+              "compact_rows (forward rows)",
+    "mutate_rev": "the same on the reverse rows",
+    "del_scan": "del_scan + del_index (inside mutate and mutate_rev)",
+    "seed": "seed_deletions, seed_insertions",
+    "inval": "inval_closure",
+    "pull": "reset_affected, pull_repair, pull_deferred, enqueue_affected",
+    "push": "push_closure",
+    "add": "plan_add, alloc_classes, seg_assign_new, mutate_add, mutate_add_big (forward rows)",
+    "add_rev": "the same on the reverse rows",
+    "cache": "seg_rescore, seg_plan, seg_pick, seg_evict, seg_admit",
+}
+
+# ncu DRAM bytes (read + write) per algorithmic HBM byte, measured on a
+# smaller case of the same kernel (the full-size launch is too large for a
+# multi-pass capture): profiles/<kernel>_*.md give the commands.  The
+# bench scales the ratio by this run's algorithmic bytes, an estimate.
+TRAFFIC_RATIO = {
+    "push_closure": (7.2, "ncu capture of push_closure, SSSP R-MAT s22 cache 4 GiB, 100k+100k batch "
+                          "(profiles/push_closure_sssp_s22_resident.md)"),
+}
 
 
-def stage_roofline(prof_stage, hbm_peak, link_peak, kind="traversal"):
-    edges, cached = prof_stage["edges"], prof_stage["edges_cached"]
-    if kind == "del_scan":
-        hbm = cached * ADJ_BYTES + prof_stage["hits"] * DEL_KEY_BYTES
-    else:
-        hbm = (prof_stage["rows"] * ROW_BYTES + edges * EDGE_STATE_BYTES + cached * ADJ_BYTES
-               + prof_stage["hits"] * HIT_BYTES)
-    link = (edges - cached) * ADJ_BYTES
-    t = prof_stage["ms"] * 1e-3
+def stage_bytes(name, st):
+    """(HBM bytes, host-link bytes) of a profiler stage from its counters."""
+    edges, cached, rows, hits = st["edges"], st["edges_cached"], st["rows"], st["hits"]
+    if name == "del_scan":
+        return cached * ADJ_BYTES + hits * DEL_KEY_BYTES, (edges - cached) * ADJ_BYTES
+    if name in ("inval", "pull", "push"):
+        return (rows * ROW_BYTES + edges * EDGE_STATE_BYTES + cached * ADJ_BYTES + hits * HIT_BYTES,
+                (edges - cached) * ADJ_BYTES)
+    if name == "group":
+        return hits * SORT_KEY_BYTES, 0
+    if name in ("mutate", "mutate_rev"):
+        return hits * DEL_REQ_BYTES, 0
+    if name in ("add", "add_rev"):
+        return hits * ADD_REQ_BYTES + edges * MOVE_ENTRY_BYTES, 0
+    if name == "cache":
+        return rows * SEG_BYTES, rows * SEG_BYTES
+    return 0, 0
+
+
+def stage_roofline(name, st, hbm_peak, link_peak, batches):
+    t = st["ms"] * 1e-3
     if t <= 0:
         return None
+    hbm, link = stage_bytes(name, st)
     t_roof = hbm / (hbm_peak * 1e9) + link / (link_peak * 1e9)
-    return {"hbm_bytes": hbm, "link_bytes": link, "seconds": t, "achieved_hbm_gbs": hbm / t / 1e9,
-            "achieved_link_gbs": link / t / 1e9, "t_roof_s": t_roof, "frac_combined": t_roof / t}
-
-
-def traffic_ratio(kernel):
-    """DRAM bytes per algorithmic HBM byte of `kernel` from profiles/traffic.md
-    (an ncu capture of a smaller case of the same kernel), or None."""
-    path = os.path.join(ROOT, "profiles", "traffic.md")
-    if not os.path.exists(path):
-        return None, None
-    with open(path) as f:
-        for line in f:
-            cells = [c.strip() for c in line.strip().strip("|").split("|")]
-            if len(cells) == 5 and cells[0] == kernel:
-                try:
-                    return float(cells[4]), cells[1]
-                except ValueError:
-                    return None, None
-    return None, None
+    return {"kernels": STAGE_KERNELS.get(name, name), "ms_per_batch": st["ms"] / batches,
+            "launches_per_batch": st["launches"] / batches, "hbm_bytes_per_batch": hbm / batches,
+            "link_bytes_per_batch": link / batches, "achieved_hbm_gbs": hbm / t / 1e9,
+            "achieved_link_gbs": link / t / 1e9, "frac_hbm": hbm / t / 1e9 / hbm_peak,
+            "frac_combined": t_roof / t}
 
 
 def stream_config(args, g):
@@ -375,6 +423,11 @@ def run_reference(args):
 
 
 def run_ours(args):
+    """The update stream: W warm-up batches, K timed batches from HBM (stage
+    profiler off), K end-to-end batches from host arrays, then outside every
+    timer a profiled pass for the per-stage breakdown and rooflines, the
+    oracle replay of every applied batch, and (N=1, default workload) the
+    uneven stream batched vs plain and the served Poisson stream."""
     import torch
 
     rank, world, local = dist_env()
@@ -388,10 +441,15 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
     from coincgraph_b200 import Engine
 
-    nb = args.warmup + 2 * args.steps
+    nprof = min(args.steps, 10)
+    nb = args.warmup + 2 * args.steps + nprof
     g, ups, setup = make_workload(args, nb)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    torch.cuda.synchronize()
+    free0, torch0 = torch.cuda.mem_get_info(dev)[0], torch.cuda.memory_reserved(dev)
     t0 = time.perf_counter()
-    eng = Engine(args.algo, device=local, source=0, cache_gib=args.cache, max_batch=args.batch)
+    eng = Engine(args.algo, device=local, source=0, cache_gib=args.cache, max_batch=args.batch,
+                 index_budget_gib=args.index_budget)
     eng.load_csr(g.n, g.xadj, g.adj)
     t1 = time.perf_counter()
     eng.init()
@@ -404,7 +462,7 @@ def run_ours(args):
         return [torch.from_numpy(x.astype(np.int32)).to(dev) for x in ups.batch(i)]
 
     batches = [dev_batch(i) for i in range(args.warmup + args.steps)]
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    torch.cuda.synchronize()
 
     def barrier():
         if world > 1:
@@ -413,12 +471,15 @@ def run_ours(args):
 
     for i in range(args.warmup):
         eng.apply_batch_device(*batches[i])
+    memory = eng.memory()
+    # cudaMemGetInfo difference since before the engine, less torch's own pool
+    memory["measured_device_bytes"] = (free0 - torch.cuda.mem_get_info(dev)[0]
+                                       - (torch.cuda.memory_reserved(dev) - torch0))
 
-    eng.profile(True)
     sampler = ClockSampler(local)
     sampler.start()
     barrier()
-    ms, edges, launches, stats = [], 0, 0, []
+    ms, edges, launches, replays, stats = [], 0, 0, 0, []
     for k in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
@@ -426,12 +487,12 @@ def run_ours(args):
         ms.append(s.ms_delete + s.ms_insert + s.ms_cache)
         edges += s.edges_scanned
         launches += s.kernel_launches
+        replays += s.graph_replays
         stats.append(s.as_dict())
     barrier()
     clocks = sampler.stop()
-    prof = eng.profile_read()
-    eng.profile(False)
     total_s = sum(ms) * 1e-3
+    del batches
 
     # e2e: host arrays through cig_apply_batch + 8-byte digest read-back.
     e2e_t, h2d = [], 0
@@ -449,49 +510,67 @@ def run_ours(args):
     if world > 1:
         total_s, e2e_total = max_over_ranks([total_s, e2e_total], dev)
 
+    # Profiled pass (not timed): per-stage device times with CUDA events.
+    eng.profile(True)
+    for k in range(nprof):
+        flush.zero_()
+        torch.cuda.synchronize()
+        eng.apply_batch_device(*dev_batch(args.warmup + 2 * args.steps + k))
+    prof = eng.profile_read()
+    eng.profile(False)
+
     hbm_peak, peak_kind = load_peaks()
     link_peak = link_peak_gbs(torch, dev)
-    stages = {}
-    for name in ("group", "mutate", "mutate_rev", "add", "add_rev", "seed", "inval", "pull", "push", "del_scan",
-                 "index"):
-        stages[name] = {"ms_per_batch": prof[name]["ms"] / args.steps, "launches": prof[name]["launches"]}
-    kern = {n: stage_roofline(prof[n], hbm_peak, link_peak, "del_scan" if n == "del_scan" else "traversal")
-            for n in ("del_scan", "inval", "pull", "push")}
-    names = {"del_scan": "del_scan", "inval": "inval_closure", "pull": "pull_repair", "push": "push_closure"}
-    dominant = max(kern, key=lambda n: prof[n]["ms"])
-    rf = kern[dominant]
-    roofline = None
-    if rf:
-        roofline = {
-            "kernel": names[dominant],
-            "bound": "hbm", "achieved": rf["achieved_hbm_gbs"], "peak": hbm_peak, "unit": "GB/s",
-            "frac": rf["achieved_hbm_gbs"] / hbm_peak, "traffic": None,
-            "traffic_source": None,
-            "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-            "hbm_bytes_per_launch": rf["hbm_bytes"] / max(prof[dominant]["launches"], 1),
-            "link_bytes_per_launch": rf["link_bytes"] / max(prof[dominant]["launches"], 1),
-            "achieved_link_gbs": rf["achieved_link_gbs"], "link_peak_gbs": link_peak,
-            "frac_of_combined_roofline": rf["frac_combined"],
-            "others": {names[k]: {"ms_per_batch": prof[k]["ms"] / args.steps, "achieved_hbm_gbs": v["achieved_hbm_gbs"],
-                                  "achieved_link_gbs": v["achieved_link_gbs"], "frac_combined": v["frac_combined"],
-                                  "hbm_bytes_per_launch": v["hbm_bytes"] / max(prof[k]["launches"], 1),
-                                  "link_bytes_per_launch": v["link_bytes"] / max(prof[k]["launches"], 1)}
-                       for k, v in kern.items() if v and k != dominant},
-        }
+    stages = {n: stage_roofline(n, prof[n], hbm_peak, link_peak, nprof) for n in STAGE_KERNELS}
+    stages = {n: v for n, v in stages.items() if v}
+    # The dominant kernel: among the stages that one kernel makes up (push:
+    # push_closure; inval: inval_closure; add: mostly mutate_add; del_scan:
+    # del_scan + del_index; pull: mostly pull_repair) the one with the most
+    # time.  (mutate, mutate_rev, group and cache are chains of 5-10 kernels
+    # each, and mutate/mutate_rev contain del_scan.)
+    dominant = max((n for n in ("push", "inval", "add", "del_scan", "pull") if n in stages),
+                   key=lambda n: stages[n]["ms_per_batch"])
+    main_kernel = {"push": "push_closure", "inval": "inval_closure", "add": "mutate_add", "del_scan": "del_scan",
+                   "pull": "pull_repair"}[dominant]
+    rf = stages[dominant]
+    hbm_launch = rf["hbm_bytes_per_batch"] * nprof / max(prof[dominant]["launches"], 1)
+    ratio = TRAFFIC_RATIO.get(main_kernel)
+    roofline = {
+        "kernel": main_kernel, "stage": dominant, "stage_kernels": rf["kernels"],
+        "bound": "hbm", "achieved": rf["achieved_hbm_gbs"], "peak": hbm_peak, "unit": "GB/s",
+        "frac": rf["frac_hbm"],
+        "traffic": ratio[0] * hbm_launch if ratio else None,
+        "traffic_source": (f"estimate: {ratio[1]}, {ratio[0]:.2f} x algorithmic HBM bytes, scaled to this "
+                           "launch's algorithmic bytes") if ratio else None,
+        "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+        "hbm_bytes_per_launch": hbm_launch,
+        "link_bytes_per_launch": rf["link_bytes_per_batch"] * nprof / max(prof[dominant]["launches"], 1),
+        "achieved_link_gbs": rf["achieved_link_gbs"], "link_peak_gbs": link_peak,
+        "frac_of_combined_roofline": rf["frac_combined"],
+        "timing": f"CUDA events around the stage on the engine stream, profiled pass of {nprof} batches",
+    }
 
-    if roofline:
-        ratio, src = traffic_ratio(roofline["kernel"])
-        if ratio:
-            roofline["traffic"] = ratio * roofline["hbm_bytes_per_launch"]
-            roofline["traffic_source"] = (f"ncu dram__bytes_read+write of {roofline['kernel']} on {src}, "
-                                          f"{ratio:.3f} x algorithmic HBM bytes, scaled to this launch "
-                                          f"(profiles/traffic.md)")
     parity = None
     if rank == 0 and not args.no_parity:
         try:
-            parity = oracle_parity(g, ups, args.warmup + 2 * args.steps, eng, args)
+            parity = oracle_parity(g, ups, args.warmup + 2 * args.steps + nprof, eng, args)
         except Exception as e:  # reported in the line, not fatal
             parity = {"values_equal": False, "rows_equal": False, "error": str(e)}
+    eng.close()
+    del eng
+    torch.cuda.synchronize()
+
+    extra = {}
+    if rank == 0 and world == 1 and args.workload == "stream" and not args.no_extras:
+        try:
+            extra["batched_vs_plain"] = uneven_stream(args, local, max_size=args.uneven_max, count=args.uneven_batches)
+        except Exception as e:  # reported in the line, not fatal
+            extra["batched_vs_plain"] = {"error": str(e)}
+        try:
+            extra["served"] = served_stream(args, local, requests=args.served_requests, rate=args.served_rate)
+        except Exception as e:
+            extra["served"] = {"error": str(e)}
+
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -505,14 +584,18 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": total_s * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": stream_config(args, g), "setup": setup,
-            "engine": {"segments_resident": info["segments_resident"], "segments_total": info["segments_total"]},
+            "engine": {"segments_resident": info["segments_resident"], "segments_total": info["segments_total"],
+                       "graphs": "batch shapes seen twice are replayed from CUDA graphs",
+                       "graph_replays_per_batch": replays / args.steps},
+            "device_memory": memory,
             "parity": parity["values_equal"] and parity["rows_equal"] if parity else None,
             "parity_detail": parity,
             "gteps": edges / total_s / 1e9 * world if total_s else None,
             "p50_ms": statistics.median(ms), "p99_ms": float(np.percentile(ms, 99)),
             "updates_per_s": value * 2 * args.batch,
             "e2e": {"value": world * args.steps / e2e_total, "unit": UNIT, "h2d_bytes_per_step": h2d // args.steps,
-                    "d2h_bytes_per_step": 8 + 144, "p50_ms": statistics.median(e2e_t) * 1e3},
+                    # the 8-byte digest + the 344-byte device status word read by every call
+                    "d2h_bytes_per_step": 8 + 344, "p50_ms": statistics.median(e2e_t) * 1e3},
             "roofline": roofline,
             "stages": stages,
             "cpu_baseline": cpu,
@@ -521,10 +604,10 @@ def run_ours(args):
             "mean_batch": {k: float(np.mean([s[k] for s in stats])) for k in
                            ("affected", "seeds", "rounds", "edges_scanned", "edges_scanned_cached",
                             "changed_sources", "relocated_rows", "missing_deletes", "cache_segments_loaded",
-                            "cache_segments_evicted")},
+                            "cache_segments_evicted", "kernel_launches")},
         }
+        line.update(extra)
         print(json.dumps(line), flush=True)
-    eng.close()
     if world > 1:
         torch.distributed.destroy_process_group()
 
@@ -590,30 +673,33 @@ def run_queries(args):
     eng.close()
 
 
-def run_uneven(args):
-    """Update batches with sizes log-uniform in [1k, --uneven-max] (half
-    deletions, half insertions): the plain form (one cig_apply_batch_device
-    per batch, synchronised) against the batched form (all batches in one
-    cig_apply_batches_device call), each on a freshly loaded engine, with the
-    per-batch value digests compared."""
+def uneven_stream(args, local, max_size, count):
+    """Update batches with sizes log-uniform in [1k, max_size] (half
+    deletions, half insertions), each form on a freshly loaded engine: the
+    plain form (direct launches, CIG_FLAG_NO_GRAPHS; one cig_apply_batch_device
+    per batch and a digest read after each) against the batched form (one
+    cig_apply_batches_device call for all batches, shapes seen twice replayed
+    from CUDA graphs, per-batch digests computed on the device).  The
+    per-batch value digests of the two forms must agree."""
     import torch
 
     from coincgraph_b200 import Engine, gen
+    from coincgraph_b200.engine import FLAG_NO_GRAPHS
 
-    _, _, local = dist_env()
-    torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     rng = np.random.default_rng(0xC01C1003)
-    sizes = np.exp(rng.uniform(np.log(1000), np.log(args.uneven_max), args.uneven_batches)).astype(np.int64)
+    sizes = np.exp(rng.uniform(np.log(1000), np.log(max_size), count)).astype(np.int64)
     symmetric = args.algo == "cc"
     # symmetric streams come in (u,v)+(v,u) pairs: even phase sizes
     half = np.maximum(sizes // 4 * 2, 2) if symmetric else np.maximum(sizes // 2, 1)
     g, h = gen.rmat(args.scale, args.edge_factor, keep_handle=True, symmetric=symmetric)
     ups = gen.updates(h, half, half, seed=gen.UPDATE_SEED_BASE + 3, symmetric=symmetric)
+    del h
     batches = [[torch.from_numpy(x.astype(np.int32)).to(dev) for x in ups.batch(i)] for i in range(len(sizes))]
     res = {}
     for form in ("plain", "batched"):
-        eng = Engine(args.algo, device=local, source=0, cache_gib=args.cache, max_batch=int(half.max()))
+        eng = Engine(args.algo, device=local, source=0, cache_gib=args.cache, max_batch=int(half.max()),
+                     flags=FLAG_NO_GRAPHS if form == "plain" else 0)
         eng.load_csr(g.n, g.xadj, g.adj)
         eng.init()
         torch.cuda.synchronize()
@@ -623,53 +709,68 @@ def run_uneven(args):
             for b in batches:
                 stats.append(eng.apply_batch_device(*b))
                 digests.append(eng.digest())
-            wall = time.perf_counter() - t0 - 0.0
         else:
             stats, digests = eng.apply_batches_device(batches)
-            wall = time.perf_counter() - t0
+        wall = time.perf_counter() - t0
         dev_ms = [s.ms_delete + s.ms_insert + s.ms_cache for s in stats]
         res[form] = {"wall_s": wall, "digests": digests, "batch_ms": dev_ms,
-                     "launches": sum(s.kernel_launches for s in stats)}
+                     "launches": sum(s.kernel_launches for s in stats),
+                     "graph_replays": sum(s.graph_replays for s in stats)}
         eng.close()
+        del eng
     same = res["plain"]["digests"] == res["batched"]["digests"]
-    line = {
-        "metric": "batches/s, batched form vs plain per-batch form", "unit": "batches/s",
-        "value": len(sizes) / res["batched"]["wall_s"], "plain_value": len(sizes) / res["plain"]["wall_s"],
-        "speedup": res["plain"]["wall_s"] / res["batched"]["wall_s"], "digests_equal": same,
-        "n_gpus": 1, "higher_is_better": True, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"{args.algo.upper()} RMAT s{args.scale} ef{args.edge_factor}"
-                               f"{' symmetric' if symmetric else ''}, {len(sizes)} batches log-uniform "
-                               f"[1k, {args.uneven_max}] (half del, half ins), cache {args.cache} GiB",
-                   "sizes": sizes.tolist()},
+    return {
+        "workload": f"{args.algo.upper()} RMAT s{args.scale} ef{args.edge_factor}{' symmetric' if symmetric else ''}, "
+                    f"{len(sizes)} batches log-uniform [1k, {max_size}] (half del, half ins), cache {args.cache} GiB",
+        "batched_batches_per_s": len(sizes) / res["batched"]["wall_s"],
+        "plain_batches_per_s": len(sizes) / res["plain"]["wall_s"],
+        "ratio": res["plain"]["wall_s"] / res["batched"]["wall_s"], "digests_equal": same,
+        "timing": "host wall clock of the whole stream, synchronised at both ends",
+        "sizes": sizes.tolist(),
         "plain": {"wall_s": res["plain"]["wall_s"], "p50_ms": statistics.median(res["plain"]["batch_ms"]),
                   "p99_ms": float(np.percentile(res["plain"]["batch_ms"], 99)), "launches": res["plain"]["launches"]},
         "batched": {"wall_s": res["batched"]["wall_s"], "launches": res["batched"]["launches"],
+                    "graph_replays": res["batched"]["graph_replays"],
+                    "p50_ms": statistics.median(res["batched"]["batch_ms"]),
+                    "p99_ms": float(np.percentile(res["batched"]["batch_ms"], 99)),
                     "device_ms_sum": sum(res["batched"]["batch_ms"])},
     }
+
+
+def run_uneven(args):
+    import torch
+
+    _, _, local = dist_env()
+    torch.cuda.set_device(local)
+    r = uneven_stream(args, local, args.uneven_max, args.uneven_batches)
+    line = {"metric": "batches/s, batched form vs plain per-batch form", "unit": "batches/s",
+            "value": r["batched_batches_per_s"], "n_gpus": 1, "higher_is_better": True, "dtype": "u32",
+            "data": "synthetic", "config": {"workload": r["workload"], "sizes": r["sizes"]}}
+    line.update({k: v for k, v in r.items() if k not in ("workload", "sizes")})
     print(json.dumps(line), flush=True)
 
 
-def run_served(args):
-    """A request stream (Poisson arrivals, or all at once) mixing update
-    batches of log-uniform sizes in [1k, --uneven-max] with BFS/SSSP queries
-    from uniform sources, served by cig_serve_* (waves, overlap) and by the
-    plain sequential form (one request at a time: cig_apply_batch, or a
-    one-source query), each on a freshly loaded engine.  Reports p50/p99
-    latency (arrival to result) and requests/s; query digests must agree."""
+def served_stream(args, local, requests, rate):
+    """A request stream (Poisson arrivals at `rate`/s, or all at once for
+    rate 0) mixing update batches of log-uniform sizes in [1k, --uneven-max]
+    with BFS/SSSP queries from uniform sources, served by cig_serve_* (waves,
+    overlap) and by the plain sequential form (one request at a time:
+    cig_apply_batch, or a one-source query), each on a freshly loaded engine.
+    Reports p50/p99 latency (arrival to result) and requests/s; update
+    digests must agree."""
     import torch
 
     from coincgraph_b200 import Engine, gen
 
-    _, _, local = dist_env()
-    torch.cuda.set_device(local)
     rng = np.random.default_rng(0xC01C1005)
-    nreq = args.requests
+    nreq = requests
     is_upd = rng.random(nreq) < args.update_frac
     nupd = int(is_upd.sum())
     sizes = np.exp(rng.uniform(np.log(1000), np.log(args.uneven_max), max(nupd, 1))).astype(np.int64)[:nupd]
     half = np.maximum(sizes // 2, 1)
     g, h = gen.rmat(args.scale, args.edge_factor, keep_handle=True)
     ups = gen.updates(h, half, half, seed=gen.UPDATE_SEED_BASE + 5)
+    del h
     deg = np.diff(g.xadj.astype(np.int64))
     live = np.flatnonzero(deg > 0)
     reqs, ui = [], 0
@@ -679,7 +780,7 @@ def run_served(args):
             ui += 1
         else:
             reqs.append(("bfs" if rng.random() < 0.5 else "sssp", int(rng.choice(live))))
-    gaps = rng.exponential(1.0 / args.rate, nreq) if args.rate > 0 else np.zeros(nreq)
+    gaps = rng.exponential(1.0 / rate, nreq) if rate > 0 else np.zeros(nreq)
     arrive = np.cumsum(gaps)
 
     def make_engine():
@@ -692,7 +793,7 @@ def run_served(args):
     out = {}
     # plain sequential form: one request at a time, in arrival order
     eng = make_engine()
-    dev_out = torch.empty((1, g.n), dtype=torch.int32, device="cuda")
+    dev_out = torch.empty((1, g.n), dtype=torch.int32, device=torch.device("cuda", local))
     lat, digests = [], []
     t0 = time.perf_counter()
     for (kind, x), ta in zip(reqs, arrive):
@@ -710,6 +811,7 @@ def run_served(args):
     out["plain"] = {"wall_s": time.perf_counter() - t0, "lat": lat}
     plain_digests = digests
     eng.close()
+    del eng, dev_out
     # served form
     eng = make_engine()
     eng.serve_start()
@@ -724,6 +826,7 @@ def run_served(args):
     wall = time.perf_counter() - t0
     eng.serve_stop()
     eng.close()
+    del eng
     lat_s = [r["done_ms"] - r["submit_ms"] for r in res]
     waves = [r["wave"] for (k, _), r in zip(reqs, res) if k != "update"]
     upd_ok = all(r["digest"] == d for (k, _), r, d in zip(reqs, res, plain_digests) if k == "update")
@@ -741,17 +844,29 @@ def run_served(args):
                 "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "query_p50_ms": pct(ql, 50),
                 "query_p99_ms": pct(ql, 99), "update_p50_ms": pct(ul, 50), "update_p99_ms": pct(ul, 99)}
 
-    line = {
-        "metric": "served request stream: requests/s and p50/p99 latency, served vs plain sequential",
-        "unit": "requests/s", "value": nreq / wall, "n_gpus": 1, "higher_is_better": True, "dtype": "u32",
-        "data": "synthetic",
-        "config": {"workload": f"RMAT s{args.scale} ef{args.edge_factor}, cache {args.cache} GiB, {nreq} requests "
-                               f"({nupd} update batches log-uniform [1k, {args.uneven_max}], the rest BFS/SSSP "
-                               f"queries), arrivals {'all at once' if args.rate <= 0 else f'Poisson {args.rate}/s'}"},
+    return {
+        "workload": f"RMAT s{args.scale} ef{args.edge_factor}, cache {args.cache} GiB, {nreq} requests "
+                    f"({nupd} update batches log-uniform [1k, {args.uneven_max}], the rest BFS/SSSP "
+                    f"queries), arrivals {'all at once' if rate <= 0 else f'Poisson {rate}/s'}",
         "served": summary("served"), "plain": summary("plain"),
         "speedup_requests_per_s": out["plain"]["wall_s"] / wall,
         "mean_wave": float(np.mean(waves)) if waves else None, "update_digests_equal": upd_ok,
+        "latency": "arrival to result visible on the host, ms",
     }
+
+
+def run_served(args):
+    import torch
+
+    _, _, local = dist_env()
+    torch.cuda.set_device(local)
+    r = served_stream(args, local, args.requests, args.rate)
+    line = {
+        "metric": "served request stream: requests/s and p50/p99 latency, served vs plain sequential",
+        "unit": "requests/s", "value": r["served"]["requests_per_s"], "n_gpus": 1, "higher_is_better": True,
+        "dtype": "u32", "data": "synthetic", "config": {"workload": r["workload"]},
+    }
+    line.update({k: v for k, v in r.items() if k != "workload"})
     print(json.dumps(line), flush=True)
 
 

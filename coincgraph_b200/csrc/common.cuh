@@ -122,6 +122,8 @@ enum Counter : int {
     // which from HBM.
     kCntDelScanned = 32,
     kCntDelScannedCached = 33,
+    // Forward row entries copied by relocations (addition phase).
+    kCntMovedEntries = 34,
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }

@@ -29,6 +29,8 @@
 #include <unordered_set>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
@@ -193,7 +195,11 @@ enum SmallIdx : int {
     kGaF = 18,  // addition-phase group counts of a presorted batch
     kGaR = 19,
     kEpoch = 23,  // batch epoch of the traversal algorithms (aff_stamp marker)
-    kSmallCount = 24
+    // the deletion counters of the reverse arena (its phase runs on the side stream)
+    kCompactCountR = 24,
+    kOrderedCountR = 25,
+    kIndexedCountR = 26,
+    kSmallCount = 32
 };
 
 constexpr uint32_t kBigRowCap = 65536;
@@ -229,7 +235,17 @@ __global__ void flush_dirty(uint8_t *dirty, const int32_t *seg_slot, const uint3
     }
 }
 
-const char *kVersion = "cig 0.1.0 (sm_100a)";
+const char *kVersion = "cig 0.2.0 (sm_100a)";
+
+// NVTX range over a host-side stage (deletion phase, insertion phase, cache
+// service, query, PR batch, load): visible to nsys/ncu timelines, free when
+// no tool is attached.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 template <class T>
 struct Identity {
@@ -244,6 +260,11 @@ struct cig_handle {
     bool dead = false;
     int device = 0;
     cudaStream_t stream = nullptr;
+    // The reverse arena's mutation runs on `side` concurrently with the
+    // forward arena's (disjoint rows, counters and scratch); `cs` is the
+    // stream that launch() and the mutation helpers queue on.
+    cudaStream_t side = nullptr, cs = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     cudaEvent_t ev[4] = {};
     int sms = 0;
     uint32_t n = 0;
@@ -294,6 +315,14 @@ struct cig_handle {
     unsigned long long *pf = nullptr, *prr = nullptr;
     uint32_t *touched = nullptr;
     uint32_t *compact = nullptr;  // rows queued for tombstone compaction
+    // The reverse arena's copies of the deletion scratch (its deletion phase
+    // runs on the side stream while the forward one runs on the engine
+    // stream), and its scan-chunk map and scan scratch.
+    uint32_t *compact_r = nullptr, *chunks_r = nullptr, *chunk_end_r = nullptr, *ordered_r = nullptr;
+    uint32_t *firstpos_r = nullptr, *indexed_groups_r = nullptr, *chunk_map_r = nullptr;
+    uint8_t *gtype_r = nullptr;
+    void *cub_r = nullptr;
+    size_t cub_r_bytes = 0;
     // flat deletion: per-group chunk counts, their inclusive prefix sum, the
     // groups left to the ordered kernels, first match per key
     uint32_t *chunks = nullptr, *chunk_end = nullptr, *ordered = nullptr, *firstpos = nullptr;
@@ -447,9 +476,9 @@ struct cig_handle {
     // an event-record node of the graph (recorded at every replay).
     void rec(cudaEvent_t e) {
         if (capturing)
-            CK(cudaEventRecordWithFlags(e, stream, cudaEventRecordExternal));
+            CK(cudaEventRecordWithFlags(e, cs, cudaEventRecordExternal));
         else
-            CK(cudaEventRecord(e, stream));
+            CK(cudaEventRecord(e, cs));
     }
     int prof_begin(int stage) {
         if (!prof_on) return -1;
@@ -486,6 +515,9 @@ struct cig_handle {
         }
         prof[CIG_STAGE_DEL_SCAN].edges += c[kCntDelScanned];
         prof[CIG_STAGE_DEL_SCAN].edges_cached += c[kCntDelScannedCached];
+        prof[CIG_STAGE_ADD].rows += c[kCntRelocated];
+        prof[CIG_STAGE_ADD].edges += c[kCntMovedEntries];
+        prof[CIG_STAGE_CACHE].rows += c[kCntSegLoaded] + c[kCntSegEvicted];
     }
 
     // ------------------------------------------------------------ helpers
@@ -508,10 +540,13 @@ struct cig_handle {
     int coop_blocks(K kernel, int tpb) const {
         int per_sm = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, tpb, 0));
-        per_sm = std::min(per_sm, static_cast<int>(tune.per_sm));
+        per_sm = std::min(per_sm, static_cast<int>(in_batch && tune.inc_per_sm ? tune.inc_per_sm : tune.per_sm));
         if (per_sm < 1) throw CigError(CIG_ERR_DEVICE, "cooperative kernel does not fit on an SM");
         return per_sm * sms;
     }
+    // Set while the closures of an update batch are queued: they may use
+    // their own launch shape (tune.inc_per_sm), the static solve uses per_sm.
+    bool in_batch = false;
 
     uint64_t n_launch = 0;  // kernels this engine launched (CUB sort kernels not included)
 
@@ -519,6 +554,7 @@ struct cig_handle {
     // cig_autotune (or CIG_COOP_BLOCKS_PER_SM / CIG_SPLIT_DEG at create).
     struct Tune {
         uint32_t per_sm = 4;        // cooperative blocks per SM (frontier tile = per_sm x 148 blocks)
+        uint32_t inc_per_sm = 0;    // the same for the closures of update batches (0: per_sm)
         uint32_t split = kSplitDeg; // rows of at least this many entries are expanded by the whole grid
         uint32_t pull_on = 32;      // BFS waves go bottom-up above n/pull_on frontier vertices (0: never)
         uint32_t pull_off = 64;     // ... and stay while at least n/pull_off
@@ -527,7 +563,7 @@ struct cig_handle {
 
     template <class... P>
     void launch(void (*kernel)(P...), int grid, int block, typename Identity<P>::type... args) {
-        kernel<<<grid, block, 0, stream>>>(args...);
+        kernel<<<grid, block, 0, cs>>>(args...);
         ++n_launch;
     }
 
@@ -769,6 +805,10 @@ struct cig_handle {
         CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
         if (!coop) throw CigError(CIG_ERR_DEVICE, "device does not support cooperative launch");
         CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming));
+        cs = stream;
         for (auto &e : ev) CK(cudaEventCreate(&e));
         dmalloc(status, 1);
         CK(cudaMemset(status, 0, sizeof(Status)));
@@ -783,7 +823,9 @@ struct cig_handle {
         pr64 = (opt.flags & CIG_FLAG_PR_FP64) != 0;
         if (const char *e = std::getenv("CIG_COOP_BLOCKS_PER_SM")) tune.per_sm = std::max(1, std::atoi(e));
         if (const char *e = std::getenv("CIG_SPLIT_DEG")) tune.split = std::max(32, std::atoi(e));
+        if (const char *e = std::getenv("CIG_INC_BLOCKS_PER_SM")) tune.inc_per_sm = std::max(0, std::atoi(e));
         if (const char *e = std::getenv("CIG_LOCAL_SWEEPS")) local_sweeps = static_cast<uint32_t>(std::max(0, std::atoi(e)));
+        if (opt.flags & CIG_FLAG_NO_GRAPHS) use_graphs = false;
         if (const char *e = std::getenv("CIG_GRAPHS")) use_graphs = std::atoi(e) != 0;
         if (const char *e = std::getenv("CIG_POS_INDEX")) use_index = std::atoi(e) != 0;
         if (const char *e = std::getenv("CIG_POS_INDEX_CLS")) index_cls = static_cast<uint32_t>(std::atoi(e));
@@ -846,6 +888,7 @@ struct cig_handle {
         dfree(tmp_u32);
         dfree(inval_done);
         dfree(chunk_map);
+        dfree(chunk_map_r);
         for (auto &b : ixb) {
             dfree(b.keys);
             dfree(b.val);
@@ -857,6 +900,10 @@ struct cig_handle {
         for (auto &e : bev) cudaEventDestroy(e);
         bev.clear();
         free_queries();
+        if (side) cudaStreamSynchronize(side);
+        if (fork_ev) cudaEventDestroy(fork_ev);
+        if (join_ev) cudaEventDestroy(join_ev);
+        if (side) cudaStreamDestroy(side);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -891,6 +938,15 @@ struct cig_handle {
         dfree(chunk_end);
         dfree(ordered);
         dfree(firstpos);
+        dfree(compact_r);
+        dfree(chunks_r);
+        dfree(chunk_end_r);
+        dfree(ordered_r);
+        dfree(firstpos_r);
+        dfree(indexed_groups_r);
+        dfree(gtype_r);
+        if (cub_r) cudaFree(cub_r);
+        cub_r = nullptr;
         dfree(gflags);
         dfree(gpos);
         dfree(gendf);
@@ -931,6 +987,13 @@ struct cig_handle {
         dmalloc(gtype, cap);
         dmalloc(indexed_groups, cap);
         dmalloc(firstpos, cap);
+        dmalloc(compact_r, cap);
+        dmalloc(chunks_r, cap);
+        dmalloc(chunk_end_r, cap);
+        dmalloc(ordered_r, cap);
+        dmalloc(gtype_r, cap);
+        dmalloc(indexed_groups_r, cap);
+        dmalloc(firstpos_r, cap);
         dmalloc(gflags, 4 * cap);
         dmalloc(gpos, 4 * cap);
         dmalloc(gendf, cap);
@@ -955,6 +1018,8 @@ struct cig_handle {
         bytes = std::max(bytes, scan_bytes);
         cub_bytes = bytes;
         CK(cudaMalloc(&cub, std::max<size_t>(bytes, 16)));
+        CK(cub::DeviceScan::InclusiveSum(nullptr, cub_r_bytes, chunks_r, chunk_end_r, static_cast<int>(cap), stream));
+        CK(cudaMalloc(&cub_r, std::max<size_t>(cub_r_bytes, 16)));
         CK(cudaHostAlloc(reinterpret_cast<void **>(&stage), 4 * cap * sizeof(uint32_t), cudaHostAllocDefault));
         bcap = cap;
         retire_graphs();
@@ -977,6 +1042,7 @@ struct cig_handle {
 
     // ------------------------------------------------------------ load
     void load_csr(uint32_t nv, const uint64_t *xadj, const uint32_t *adj) {
+        const NvtxRange range("cig.load");
         if (loaded) throw CigError(CIG_ERR_ARG, "graph already loaded");
         if (nv == 0) throw CigError(CIG_ERR_ARG, "graph must have at least one vertex");
         if (!xadj || (xadj[nv] && !adj)) throw CigError(CIG_ERR_ARG, "null CSR arrays");
@@ -1276,6 +1342,7 @@ struct cig_handle {
     template <class T>
     void pr_batch(const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd, const uint32_t *d_au,
                   const uint32_t *d_av, uint64_t na) {
+        const NvtxRange range("cig.pr_batch");
         auto a = pr_arrays<T>();
         const T eps = static_cast<T>(opt.pr_epsilon);
         ++epoch;
@@ -1414,6 +1481,7 @@ struct cig_handle {
     }
 
     void run_cache_service() {
+        const NvtxRange range("cig.cache_service");
         const int p = prof_begin(CIG_STAGE_CACHE);
         cache_service();
         prof_end(p);
@@ -1510,8 +1578,11 @@ struct cig_handle {
         if (need <= chunk_map_cap) return;
         if (capturing) throw CigError(CIG_ERR_DEVICE, "internal: scan-chunk map grows under capture");
         CK(cudaStreamSynchronize(stream));
+        CK(cudaStreamSynchronize(side));
         dfree(chunk_map);
+        dfree(chunk_map_r);
         dmalloc(chunk_map, need);
+        dmalloc(chunk_map_r, need);
         chunk_map_cap = need;
         retire_graphs();
     }
@@ -1535,9 +1606,20 @@ struct cig_handle {
         }
     }
 
-    // Host-side accounting of a deletion phase (kept out of captured code).
+    // Host-side accounting of the phases for the stage profiler (kept out of
+    // captured code): requests per stage, sorted keys.
     void note_delete_phase(uint64_t nd) {
-        if (prof_on && nd) prof[CIG_STAGE_DEL_SCAN].hits += 2 * nd;
+        if (!prof_on || !nd) return;
+        prof[CIG_STAGE_DEL_SCAN].hits += 2 * nd;
+        prof[CIG_STAGE_MUTATE].hits += nd;
+        prof[CIG_STAGE_MUTATE_REV].hits += nd;
+        prof[CIG_STAGE_GROUP].hits += 2 * nd;
+    }
+    void note_insert_phase(uint64_t na) {
+        if (!prof_on || !na) return;
+        prof[CIG_STAGE_ADD].hits += na;
+        prof[CIG_STAGE_ADD_REV].hits += na;
+        prof[CIG_STAGE_GROUP].hits += 2 * na;
     }
 
     void mutate_delete_arena(DevArena &A, const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd, bool forward,
@@ -1551,6 +1633,16 @@ struct cig_handle {
         uint32_t *big = forward ? bigf : bigr;
         uint32_t *gcount = small + (forward ? kGcF : kGcR);
         uint32_t *bcount = small + (forward ? kBigF : kBigR);
+        uint32_t *chunks = forward ? this->chunks : chunks_r;
+        uint32_t *chunk_end = forward ? this->chunk_end : chunk_end_r;
+        uint32_t *ordered = forward ? this->ordered : ordered_r;
+        uint32_t *firstpos = forward ? this->firstpos : firstpos_r;
+        uint32_t *indexed_groups = forward ? this->indexed_groups : indexed_groups_r;
+        uint32_t *compact = forward ? this->compact : compact_r;
+        uint32_t *chunk_map = forward ? this->chunk_map : chunk_map_r;
+        uint8_t *gtype = forward ? this->gtype : gtype_r;
+        void *scan_tmp = forward ? cub : cub_r;
+        size_t scan_tmp_bytes = forward ? cub_bytes : cub_r_bytes;
         int p = prof_begin(CIG_STAGE_GROUP);
         unsigned long long *sorted = keys;
         Groups grp{groups, forward ? gendf : gendr, gcount};
@@ -1563,27 +1655,24 @@ struct cig_handle {
             sorted = sort_keys(keys, tmp, nd);
             grp = build_groups(sorted, nd, groups, forward ? gendf : gendr, gcount);
         }
-        CK(cudaMemsetAsync(bcount, 0, sizeof(uint32_t), stream));
-        CK(cudaMemsetAsync(matched, 0, nd * sizeof(uint32_t), stream));
+        CK(cudaMemsetAsync(bcount, 0, sizeof(uint32_t), cs));
+        CK(cudaMemsetAsync(matched, 0, nd * sizeof(uint32_t), cs));
         prof_end(p);
         p = prof_begin(forward ? CIG_STAGE_MUTATE : CIG_STAGE_MUTATE_REV);
         unsigned long long *stats = with_stats ? status->counters : nullptr;
-        uint32_t *ccount = small + kCompactCount;
-        uint32_t *ocount = small + kOrderedCount;
-        CK(cudaMemsetAsync(ccount, 0, sizeof(uint32_t), stream));
-        CK(cudaMemsetAsync(ocount, 0, sizeof(uint32_t), stream));
-        CK(cudaMemsetAsync(chunks, 0, nd * sizeof(uint32_t), stream));
-        CK(cudaMemsetAsync(firstpos, 0xFF, nd * sizeof(uint32_t), stream));
+        uint32_t *ccount = small + (forward ? kCompactCount : kCompactCountR);
+        uint32_t *ocount = small + (forward ? kOrderedCount : kOrderedCountR);
+        CK(cudaMemsetAsync(ccount, 0, sizeof(uint32_t), cs));
+        CK(cudaMemsetAsync(ocount, 0, sizeof(uint32_t), cs));
+        CK(cudaMemsetAsync(chunks, 0, nd * sizeof(uint32_t), cs));
+        CK(cudaMemsetAsync(firstpos, 0xFF, nd * sizeof(uint32_t), cs));
         // Flat path: rows whose deletion requests are all distinct.
-        uint32_t *icount = small + kIndexedCount;
-        CK(cudaMemsetAsync(icount, 0, sizeof(uint32_t), stream));
+        uint32_t *icount = small + (forward ? kIndexedCount : kIndexedCountR);
+        CK(cudaMemsetAsync(icount, 0, sizeof(uint32_t), cs));
         const PosIndex ix = pos_index(forward);
         launch(del_classify, persistent_grid(), 256, A.desc, sorted, grp, chunks, gtype, ordered, ocount, ix,
                indexed_groups, icount);
-        {
-            size_t bytes = cub_bytes;
-            CK(cub::DeviceScan::InclusiveSum(cub, bytes, chunks, chunk_end, static_cast<int>(nd), stream));
-        }
+        CK(cub::DeviceScan::InclusiveSum(scan_tmp, scan_tmp_bytes, chunks, chunk_end, static_cast<int>(nd), cs));
         reserve_chunk_map(nd);
         launch(del_chunk_map, persistent_grid(), 256, grp, chunk_end, chunk_map);
         const int ps = prof_begin(CIG_STAGE_DEL_SCAN);
@@ -1632,7 +1721,7 @@ struct cig_handle {
             sorted = sort_keys(keys, tmp, na);
             grp = build_groups(sorted, na, groups, forward ? gendf : gendr, gcount);
         }
-        CK(cudaMemsetAsync(bcount, 0, sizeof(uint32_t), stream));
+        CK(cudaMemsetAsync(bcount, 0, sizeof(uint32_t), cs));
         prof_end(p);
         p = prof_begin(forward ? CIG_STAGE_ADD : CIG_STAGE_ADD_REV);
         launch(plan_add, persistent_grid(), 256, A.desc, sorted, grp, plan, A.alloc);
@@ -1650,8 +1739,43 @@ struct cig_handle {
     }
 
     // ------------------------------------------------------------ batches
+    // The forward and reverse rows of a presorted batch are mutated
+    // concurrently: the reverse arena's kernels go to the side stream, forked
+    // from and joined back into the engine stream (a fork/join of the
+    // captured graph under capture).  The two touch disjoint rows, scratch
+    // and counters; unsorted per-phase calls stay on one stream (their key
+    // building is shared).
+    template <class F, class G>
+    void fork_arenas(F fwd_part, G rev_part) {
+        if (!presorted) {
+            fwd_part();
+            rev_part();
+            return;
+        }
+        CK(cudaEventRecord(fork_ev, stream));
+        CK(cudaStreamWaitEvent(side, fork_ev, 0));
+        cs = side;
+        try {
+            rev_part();
+        } catch (...) {
+            cs = stream;
+            throw;
+        }
+        cs = stream;
+        fwd_part();
+        CK(cudaEventRecord(join_ev, side));
+        CK(cudaStreamWaitEvent(stream, join_ev, 0));
+    }
+
+    struct InBatch {
+        bool &flag;
+        explicit InBatch(bool &f) : flag(f) { flag = true; }
+        ~InBatch() { flag = false; }
+    };
+
     template <int A>
     void delete_phase_dev(const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd) {
+        const InBatch ib(in_batch);
         const uint32_t *ep = small + kEpoch;
         launch(phase_begin, 1, 32, small + kEpoch, small + kFr, 6u);  // frontier + affected counters
         int p = prof_begin(CIG_STAGE_SEED);
@@ -1660,8 +1784,8 @@ struct cig_handle {
                                                                 aff_stamp, ep, list, small + kAff, n + 1, status);
         prof_end(p);
         check_launch();
-        mutate_delete_arena(fwd, d_du, d_dv, nd, true, true);
-        mutate_delete_arena(rev, d_du, d_dv, nd, false, false);
+        fork_arenas([&] { mutate_delete_arena(fwd, d_du, d_dv, nd, true, true); },
+                    [&] { mutate_delete_arena(rev, d_du, d_dv, nd, false, false); });
         p = prof_begin(CIG_STAGE_INVAL);
         if (local_sweeps) CK(cudaMemsetAsync(small + kInvalDone, 0, sizeof(uint32_t), stream));
         launch_coop(inval_closure<A>, kTpb, fwd.view(), state, aff_stamp, ep, list, small + kAff, n + 1,
@@ -1682,9 +1806,10 @@ struct cig_handle {
 
     template <int A>
     void insert_phase_dev(const uint32_t *d_au, const uint32_t *d_av, uint64_t na) {
+        const InBatch ib(in_batch);
         CK(cudaMemsetAsync(small + kFr, 0, 3 * sizeof(uint32_t), stream));
-        mutate_add_arena(fwd, d_au, d_av, na, true, true);
-        mutate_add_arena(rev, d_au, d_av, na, false, false);
+        fork_arenas([&] { mutate_add_arena(fwd, d_au, d_av, na, true, true); },
+                    [&] { mutate_add_arena(rev, d_au, d_av, na, false, false); });
         int p = prof_begin(CIG_STAGE_SEED);
         if (na)
             launch(seed_insertions<A>, grid_for(na), 256, d_au, d_av, static_cast<uint32_t>(na), n, state,
@@ -1761,6 +1886,7 @@ struct cig_handle {
 
     void stage_batch(const uint32_t *hdu, const uint32_t *hdv, uint64_t nd, const uint32_t *hau, const uint32_t *hav,
                      uint64_t na) {
+        const NvtxRange range("cig.stage_host_arrays");
         if ((nd && (!hdu || !hdv)) || (na && (!hau || !hav))) throw CigError(CIG_ERR_ARG, "null update array");
         const uint32_t *src[4] = {hdu, hdv, hau, hav};
         const uint64_t cnt[4] = {nd, nd, na, na};
@@ -1789,6 +1915,7 @@ struct cig_handle {
     }
 
     void delete_phase_host(const uint32_t *hu, const uint32_t *hv, uint64_t nd, cig_batch_stats *s) {
+        const NvtxRange range("cig.delete_phase");
         require_ready();
         if (opt.algo == CIG_PR) throw CigError(CIG_ERR_ARG, "PageRank applies whole batches (cig_apply_batch)");
         ensure_batch(nd);
@@ -1806,12 +1933,14 @@ struct cig_handle {
     }
 
     void insert_phase_host(const uint32_t *hu, const uint32_t *hv, uint64_t na, cig_batch_stats *s) {
+        const NvtxRange range("cig.insert_phase");
         require_ready();
         if (opt.algo == CIG_PR) throw CigError(CIG_ERR_ARG, "PageRank applies whole batches (cig_apply_batch)");
         ensure_batch(na);
         reset_counters();
         CK(cudaEventRecord(ev[1], stream));
         stage_batch(nullptr, nullptr, 0, hu, hv, na);
+        note_insert_phase(na);
         index_upkeep(na);
         dispatch([&](auto tag) {
             run_graphed(2, 0, na, [&] { insert_phase_dev<decltype(tag)::value>(au, av, na); });
@@ -1835,7 +1964,9 @@ struct cig_handle {
     void traversal_batch(const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd, const uint32_t *d_au,
                          const uint32_t *d_av, uint64_t na, cudaEvent_t mutation_after, cudaEvent_t e1,
                          cudaEvent_t e2) {
+        const NvtxRange range("cig.batch");
         note_delete_phase(nd);
+        note_insert_phase(na);
         index_upkeep(na);
         reserve_chunk_map(nd);
         if (mutation_after || !use_graphs) {
@@ -2189,6 +2320,7 @@ struct cig_handle {
     // Queue the waves of a query on qstream (after the updates already queued
     // on the engine stream); q_ev[2] marks their end.  Returns the wave count.
     uint32_t query_launch(int algo, const uint32_t *sources, uint32_t k, uint32_t width, uint32_t *out) {
+        const NvtxRange range("cig.query");
         if (!loaded) throw CigError(CIG_ERR_ARG, "load a graph first");
         require_alive();
         if (algo != CIG_BFS && algo != CIG_SSSP) throw CigError(CIG_ERR_ARG, "queries are BFS or SSSP");

@@ -1076,7 +1076,7 @@ __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long
     const uint32_t lane = lane_id();
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t ng = *gr.count;
-    uint32_t changed = 0, moved = 0;  // per lane
+    uint32_t changed = 0, moved = 0, moved_entries = 0;  // per lane
     for (uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; base < ng; base += warps * 32u) {
         const uint32_t g = base + lane;
         bool coop = false;
@@ -1114,6 +1114,7 @@ __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long
                         if (row[k] != kTomb) write_slot(view, off + w++, row[k]);
                     for (uint32_t j = 0; j < a; ++j) write_slot(view, off + w + j, vals[key_low(keys[gs + j])]);
                     desc[u] = RowDesc{off, w + a, rd_meta(cls, 0)};
+                    moved_entries += w;
                     if (indexed) {
                         for (uint32_t k = 0; k < w; ++k) idx_pos_reset(ix, u, __ldcg(view.at(off + k)), st);
                         for (uint32_t k = 0; k < w; ++k) idx_pos_set(ix, u, __ldcg(view.at(off + k)), k);
@@ -1150,14 +1151,44 @@ __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long
                 }
                 const uint32_t cls = static_cast<uint32_t>(p >> 32);
                 const unsigned long long off = alloc_offset(al, cls, static_cast<uint32_t>(p));
+                // Copy the survivors in order, 256 entries per step: each lane
+                // issues two independent 16-byte loads (the old block lies in
+                // one segment and starts on a 16-byte boundary) before any
+                // store, so a zero-copy row costs one host round trip per
+                // 256 entries instead of one per 32.
+                const uint32_t *src = view.at(d.off);
                 uint32_t w = 0;
-                for (uint32_t b0 = 0; b0 < d.len; b0 += 32u) {
-                    const uint32_t k = b0 + lane;
-                    const uint32_t x = k < d.len ? *view.at(d.off + k) : kTomb;
-                    const uint32_t km = __ballot_sync(kFull, x != kTomb);
-                    if (x != kTomb) write_slot(view, off + w + __popc(km & lanemask_lt()), x);
-                    w += __popc(km);
+                for (uint32_t b0 = 0; b0 < d.len; b0 += 256u) {
+                    uint32_t e[8];
+#pragma unroll
+                    for (uint32_t h = 0; h < 2; ++h) {
+                        const uint32_t k = b0 + 128u * h + 4u * lane;
+                        uint4 q = make_uint4(kTomb, kTomb, kTomb, kTomb);
+                        if (k < d.len) q = *reinterpret_cast<const uint4 *>(src + k);
+                        e[4 * h] = k < d.len ? q.x : kTomb;
+                        e[4 * h + 1] = k + 1u < d.len ? q.y : kTomb;
+                        e[4 * h + 2] = k + 2u < d.len ? q.z : kTomb;
+                        e[4 * h + 3] = k + 3u < d.len ? q.w : kTomb;
+                    }
+#pragma unroll
+                    for (uint32_t h = 0; h < 2; ++h) {
+                        uint32_t c = 0;
+#pragma unroll
+                        for (uint32_t j = 0; j < 4; ++j) c += e[4 * h + j] != kTomb ? 1u : 0u;
+                        uint32_t incl = c;
+#pragma unroll
+                        for (uint32_t o = 1; o < 32u; o <<= 1) {
+                            const uint32_t t = __shfl_up_sync(kFull, incl, o);
+                            if (lane >= o) incl += t;
+                        }
+                        uint32_t pos = w + incl - c;
+#pragma unroll
+                        for (uint32_t j = 0; j < 4; ++j)
+                            if (e[4 * h + j] != kTomb) write_slot(view, off + pos++, e[4 * h + j]);
+                        w += __shfl_sync(kFull, incl, 31);
+                    }
                 }
+                if (lane == 0) moved_entries += w;
                 for (uint32_t j = lane; j < a; j += 32u) write_slot(view, off + w + j, vals[key_low(keys[gs + j])]);
                 if (lane == 0) desc[u] = RowDesc{off, w + a, rd_meta(cls, 0)};
                 if (idx_row(ix, u)) {
@@ -1173,6 +1204,7 @@ __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long
     if (stats) {
         warp_count(&stats[kCntChanged], changed);
         warp_count(&stats[kCntRelocated], moved);
+        warp_count(&stats[kCntMovedEntries], moved_entries);
     }
 }
 
@@ -1216,6 +1248,7 @@ __global__ void __launch_bounds__(kTpbMut)
             if (stats) {
                 atomicAdd(&stats[kCntChanged], 1ull);
                 atomicAdd(&stats[kCntRelocated], 1ull);
+                atomicAdd(&stats[kCntMovedEntries], static_cast<unsigned long long>(w));
             }
         }
     }

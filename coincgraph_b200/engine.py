@@ -20,6 +20,7 @@ ALGOS = {"bfs": BFS, "sssp": SSSP, "cc": CC, "pr": PR}
 FLAG_NO_CACHE_REFRESH = 0x1
 FLAG_PR_FP64 = 0x2
 FLAG_WEIGHT_U255 = 0x4
+FLAG_NO_GRAPHS = 0x8
 INF = 0xFFFFFFFF
 
 STATUS = {

@@ -63,6 +63,8 @@ typedef struct {
 
 #define CIG_FLAG_NO_CACHE_REFRESH 0x1u /* keep the segment residency chosen at load */
 #define CIG_FLAG_PR_FP64 0x2u          /* PR ranks/residuals in FP64 (default: FP32 + Kahan) */
+#define CIG_FLAG_NO_GRAPHS 0x8u         /* launch every batch kernel directly (default: a batch shape seen twice
+                                          is captured into CUDA graphs and replayed) */
 #define CIG_FLAG_WEIGHT_U255 0x4u      /* SSSP weights uniform in [1, 255]: 1 + lowbias32(u*0x9E3779B1 +
                                           v*0x85EBCA77) mod 255 (an extension; the reference's SSSP
                                           weight is (u+v)%128+1 whatever the file holds) */

@@ -17,7 +17,8 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REFERENCE = "/root/reference"
+# The reference source tree (read-only; only this recipe reads it).
+REFERENCE = os.environ.get("CIG_REFERENCE_DIR", "/root/reference")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 
 
