@@ -63,6 +63,23 @@ def build_engine(force: bool = False, verbose_ptxas: bool = False) -> str:
     return out
 
 
+def build_engine_bounds_checked(force: bool = False) -> str:
+    """``libcig_bc.so``: the engine compiled with -DCIG_BOUNDS_CHECK, which
+    checks every arena slot and every vertex id read from a row against its
+    bound and reports a violation through the device status word
+    (CIG_ERR_LIMIT, "device index out of bounds") instead of touching memory
+    outside the arrays.  A test-and-debug build (slower); select it with
+    CIG_LIBRARY=<path> in the Python binding or by linking it instead of
+    libcig.so."""
+    out = os.path.join(HERE, "libcig_bc.so")
+    deps = _sources((".cu", ".cuh")) + [os.path.join(INCLUDE, "cig.h")]
+    if force or _stale(out, deps):
+        _run([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-DCIG_BOUNDS_CHECK",
+              "-Xcompiler", "-fPIC", "-shared", "-I" + INCLUDE,
+              os.path.join(CSRC, "engine.cu"), os.path.join(CSRC, "noalloc.cu"), "-o", out])
+    return out
+
+
 def build_generator(force: bool = False) -> str:
     out = os.path.join(HERE, "libcig_gen.so")
     src = os.path.join(CSRC, "graphgen.cpp")
@@ -91,6 +108,7 @@ def build_cli(force: bool = False) -> list[str]:
 def build_all(force: bool = False) -> dict:
     return {
         "engine": build_engine(force),
+        "engine_bounds_checked": build_engine_bounds_checked(force),
         "generator": build_generator(force),
         "cli": build_cli(force),
     }

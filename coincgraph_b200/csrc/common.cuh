@@ -34,6 +34,7 @@ enum : uint32_t {
     kErrBarrier = 1u << 3,   // grid barrier wait limit exceeded
     kErrNonFinite = 1u << 4, // PR produced a non-finite value
     kErrInternal = 1u << 5,
+    kErrBounds = 1u << 6,    // an index out of range (bounds-check build only)
 };
 
 // A deleted entry is overwritten with kTomb (never a vertex id: ids are
@@ -60,24 +61,57 @@ __host__ __device__ __forceinline__ uint32_t rd_meta(uint32_t cls, uint32_t tomb
 // holds the whole arena.  The cache is write-back: a resident segment's HBM
 // copy is authoritative and `seg_dirty` marks segments whose host copy is
 // stale (copied back before any host-side read or eviction).
+struct Status;
+__device__ __forceinline__ void report_bounds(Status *st, uint64_t index);
+
 struct AdjView {
     const RowDesc *desc;
     uint32_t *dev;            // cache pool (forward) or arena (device-only)
     uint32_t *host;           // mapped host arena (forward) or null
     const int32_t *seg_slot;  // null for a device-only arena
     uint8_t *seg_dirty;       // null for a device-only arena
+#ifdef CIG_BOUNDS_CHECK
+    // Bounds-check build: arena slots and vertex ids in range (0 = not
+    // checked); a violation sets kErrBounds in `bst` and the access is
+    // redirected to slot 0 / dropped, so the kernel finishes and the host
+    // reports the error.
+    uint64_t nslots = 0;
+    uint32_t nverts = 0;
+    Status *bst = nullptr;
+    __device__ __forceinline__ uint64_t chk(uint64_t off) const {
+        if (nslots && off >= nslots) {
+            report_bounds(bst, off);
+            return 0;
+        }
+        return off;
+    }
+    // A row entry used as a vertex id: out of range reads as a tombstone.
+    __device__ __forceinline__ uint32_t vid(uint32_t y) const {
+        if (nverts && y != 0xFFFFFFFFu && y >= nverts) {
+            report_bounds(bst, y);
+            return 0xFFFFFFFFu;
+        }
+        return y;
+    }
+#else
+    __device__ __forceinline__ uint64_t chk(uint64_t off) const { return off; }
+    __device__ __forceinline__ uint32_t vid(uint32_t y) const { return y; }
+#endif
 
     __device__ __forceinline__ uint32_t *at(uint64_t off) const {
+        off = chk(off);
         if (!seg_slot) return dev + off;
         const int32_t s = __ldg(seg_slot + (off >> kSegShift));
         return s >= 0 ? dev + ((static_cast<uint64_t>(s) << kSegShift) | (off & kSegMask)) : host + off;
     }
     __device__ __forceinline__ bool cached(uint64_t off) const {
+        off = chk(off);
         return !seg_slot || __ldg(seg_slot + (off >> kSegShift)) >= 0;
     }
     // The authoritative copy of slot `off` for writing; marks a resident
     // segment dirty.  Valid for the whole segment containing `off`.
     __device__ __forceinline__ uint32_t *wptr(uint64_t off) const {
+        off = chk(off);
         if (!seg_slot) return dev + off;
         const uint64_t seg = off >> kSegShift;
         const int32_t s = seg_slot[seg];
@@ -139,6 +173,10 @@ __device__ __forceinline__ uint32_t ld_volatile(const uint32_t *p) {
 
 __device__ __forceinline__ void set_error(Status *st, uint32_t code, uint32_t info = 0) {
     if ((atomicOr(&st->err, code) & code) == 0) st->err_info = info;
+}
+
+__device__ __forceinline__ void report_bounds(Status *st, uint64_t index) {
+    if (st) set_error(st, kErrBounds, static_cast<uint32_t>(index));
 }
 
 // Warp-aggregated append: one atomicAdd per warp.  All 32 lanes must call.

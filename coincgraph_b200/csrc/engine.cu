@@ -214,7 +214,17 @@ struct DevArena {
     ArenaAlloc *alloc = nullptr;
     uint64_t seg_total = 0;
     uint64_t seg_used = 0;
-    AdjView view() const { return AdjView{desc, dev, host_dptr, seg_slot, seg_dirty}; }
+    Status *bstatus = nullptr;  // bounds-check build: where violations are reported
+    uint32_t nverts = 0;
+    AdjView view() const {
+        AdjView v{desc, dev, host_dptr, seg_slot, seg_dirty};
+#ifdef CIG_BOUNDS_CHECK
+        v.nslots = seg_total * kSegEdges;
+        v.nverts = nverts;
+        v.bst = bstatus;
+#endif
+        return v;
+    }
 };
 
 // Write-back of the edge cache: copy every dirty resident segment to its
@@ -775,6 +785,7 @@ struct cig_handle {
             if (e & kErrQueue) what += "work queue overflow; ";
             if (e & kErrNonFinite) what += "non-finite PageRank value; ";
             if (e & kErrInternal) what += "internal consistency error; ";
+            if (e & kErrBounds) what += "device index out of bounds (bounds-check build); ";
             throw CigError(code, "device reported: " + what + "info=" + std::to_string(h_status->err_info));
         }
     }
@@ -1083,6 +1094,8 @@ struct cig_handle {
                                                  (1ull << 20) >> kSegShift);
         fwd.seg_used = L.used_segs;
         fwd.seg_total = L.used_segs + head;
+        fwd.nverts = n;
+        fwd.bstatus = status;
         const size_t host_bytes = fwd.seg_total * kSegEdges * sizeof(uint32_t);
         {
             const cudaError_t e = cudaHostAlloc(reinterpret_cast<void **>(&fwd.host), host_bytes,
@@ -1249,6 +1262,8 @@ struct cig_handle {
                                                  (1ull << 20) >> kSegShift);
         rev.seg_used = L.used_segs;
         rev.seg_total = L.used_segs + head;
+        rev.nverts = n;
+        rev.bstatus = status;
         dmalloc(rev.dev, rev.seg_total * kSegEdges);
         dmalloc(rev.desc, n);
         CK(cudaMemcpy(rev.desc, L.desc.data(), n * sizeof(RowDesc), cudaMemcpyHostToDevice));
@@ -1343,6 +1358,8 @@ struct cig_handle {
     void pr_batch(const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd, const uint32_t *d_au,
                   const uint32_t *d_av, uint64_t na) {
         const NvtxRange range("cig.pr_batch");
+        reserve_chunk_map(nd);
+        index_upkeep(na);
         auto a = pr_arrays<T>();
         const T eps = static_cast<T>(opt.pr_epsilon);
         ++epoch;
@@ -1625,6 +1642,7 @@ struct cig_handle {
     void mutate_delete_arena(DevArena &A, const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd, bool forward,
                              bool with_stats) {
         if (nd == 0) return;
+        reserve_chunk_map(nd);  // before the map's address is taken below
         const uint32_t m = static_cast<uint32_t>(nd);
         unsigned long long *keys = forward ? kf : kr;
         unsigned long long *tmp = forward ? t1 : t2;
@@ -1673,7 +1691,6 @@ struct cig_handle {
         launch(del_classify, persistent_grid(), 256, A.desc, sorted, grp, chunks, gtype, ordered, ocount, ix,
                indexed_groups, icount);
         CK(cub::DeviceScan::InclusiveSum(scan_tmp, scan_tmp_bytes, chunks, chunk_end, static_cast<int>(nd), cs));
-        reserve_chunk_map(nd);
         launch(del_chunk_map, persistent_grid(), 256, grp, chunk_end, chunk_map);
         const int ps = prof_begin(CIG_STAGE_DEL_SCAN);
         launch(del_scan, sms * del_scan_blocks_per_sm(), kMutWarps * 32, A.view(), A.desc, sorted, grp, chunk_end,
@@ -2319,6 +2336,16 @@ struct cig_handle {
 
     // Queue the waves of a query on qstream (after the updates already queued
     // on the engine stream); q_ev[2] marks their end.  Returns the wave count.
+    // The forward view as the query kernels see it (a bounds-check build
+    // reports into the query status word).
+    AdjView query_view() const {
+        AdjView v = fwd.view();
+#ifdef CIG_BOUNDS_CHECK
+        v.bst = qstatus;
+#endif
+        return v;
+    }
+
     uint32_t query_launch(int algo, const uint32_t *sources, uint32_t k, uint32_t width, uint32_t *out) {
         const NvtxRange range("cig.query");
         if (!loaded) throw CigError(CIG_ERR_ARG, "load a graph first");
@@ -2349,13 +2376,13 @@ struct cig_handle {
                                                  fr, qstatus);
             ++n_launch;
             if (algo == CIG_BFS)
-                launch_coop_on(qstream, ms_closure<kBfs>, kTpbMs, fwd.view(), ms_dist, width, ms_visit, fr, bl, n + 2,
+                launch_coop_on(qstream, ms_closure<kBfs>, kTpbMs, query_view(), ms_dist, width, ms_visit, fr, bl, n + 2,
                                ms_pull(kw), qstatus);
             else if (opt.flags & CIG_FLAG_WEIGHT_U255)
-                launch_coop_on(qstream, ms_closure<kSsspU>, kTpbMs, fwd.view(), ms_dist, width,
+                launch_coop_on(qstream, ms_closure<kSsspU>, kTpbMs, query_view(), ms_dist, width,
                                static_cast<unsigned long long *>(nullptr), fr, bl, n + 2, MsPull{}, qstatus);
             else
-                launch_coop_on(qstream, ms_closure<kSssp>, kTpbMs, fwd.view(), ms_dist, width,
+                launch_coop_on(qstream, ms_closure<kSssp>, kTpbMs, query_view(), ms_dist, width,
                                static_cast<unsigned long long *>(nullptr), fr, bl, n + 2, MsPull{}, qstatus);
             ms_transpose<<<(n + kMsTile - 1) / kMsTile, 256, 0, qstream>>>(ms_dist, n, width, kw,
                                                                          out + static_cast<uint64_t>(j0) * n);
@@ -2375,6 +2402,7 @@ struct cig_handle {
             if (h_qstatus->err & kErrRounds) what += "round bound exceeded; ";
             if (h_qstatus->err & kErrBarrier) what += "grid barrier wait limit exceeded; ";
             if (h_qstatus->err & kErrQueue) what += "work queue overflow; ";
+            if (h_qstatus->err & kErrBounds) what += "device index out of bounds (bounds-check build); ";
             throw CigError(CIG_ERR_LIMIT, "query: device reported: " + what + "info=" +
                                               std::to_string(h_qstatus->err_info));
         }
@@ -3077,5 +3105,25 @@ int cig_query_multi_device(cig_handle *h, int algo, const uint32_t *sources, uin
 }
 
 const char *cig_version(void) { return kVersion; }
+
+int cig_build_info(int *binary_version, int *bounds_checked) {
+    if (bounds_checked) {
+#ifdef CIG_BOUNDS_CHECK
+        *bounds_checked = 1;
+#else
+        *bounds_checked = 0;
+#endif
+    }
+    if (!binary_version) return CIG_OK;
+    cudaFuncAttributes a{};
+    const cudaError_t e = cudaFuncGetAttributes(&a, reinterpret_cast<const void *>(value_digest));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        cig_set_unbound_error(std::string("cudaFuncGetAttributes: ") + cudaGetErrorString(e));
+        return CIG_ERR_DEVICE;
+    }
+    *binary_version = a.binaryVersion;
+    return CIG_OK;
+}
 
 }  // extern "C"

@@ -83,13 +83,17 @@ struct Defer {
 // thread of the group runs the same number of steps (Op::edge is
 // warp-synchronous).
 template <uint32_t lanes, class Op, class P>
-__device__ __forceinline__ void sweep_row(const uint32_t *rp, uint32_t deg, uint32_t t, uint32_t x, P payload,
-                                          const Op &op, ExpandCounters &cnt) {
+__device__ __forceinline__ void sweep_row(const AdjView &view, const uint32_t *rp, uint32_t deg, uint32_t t,
+                                          uint32_t x, P payload, const Op &op, ExpandCounters &cnt) {
     if ((reinterpret_cast<uintptr_t>(rp) & 15u) == 0) {
         for (uint32_t base = 0; base < deg; base += 4u * lanes) {
             const uint32_t k = base + 4u * t;
             uint4 q = make_uint4(kTomb, kTomb, kTomb, kTomb);
             if (k < deg) q = __ldg(reinterpret_cast<const uint4 *>(rp + k));
+            q.x = view.vid(q.x);
+            q.y = view.vid(q.y);
+            q.z = view.vid(q.z);
+            q.w = view.vid(q.w);
             cnt.hits += op.edge(k < deg && q.x != kTomb, x, payload, q.x);
             cnt.hits += op.edge(k + 1u < deg && q.y != kTomb, x, payload, q.y);
             cnt.hits += op.edge(k + 2u < deg && q.z != kTomb, x, payload, q.z);
@@ -99,7 +103,7 @@ __device__ __forceinline__ void sweep_row(const uint32_t *rp, uint32_t deg, uint
         for (uint32_t base = 0; base < deg; base += lanes) {
             const uint32_t k = base + t;
             const bool valid = k < deg;
-            const uint32_t y = valid ? __ldg(rp + k) : 0u;
+            const uint32_t y = valid ? view.vid(__ldg(rp + k)) : 0u;
             cnt.hits += op.edge(valid && y != kTomb, x, payload, y);
         }
     }
@@ -145,12 +149,12 @@ __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint3
         const P bp = sm.b_payload;
         const uint64_t boff = sm.b_off;
         if (bdeg <= kSegEdges) {
-            sweep_row<TPB>(view.at(boff), bdeg, threadIdx.x, bx, bp, op, cnt);
+            sweep_row<TPB>(view, view.at(boff), bdeg, threadIdx.x, bx, bp, op, cnt);
         } else {
             for (uint32_t base = 0; base < bdeg; base += TPB) {
                 const uint32_t k = base + threadIdx.x;
                 const bool valid = k < bdeg;
-                const uint32_t y = valid ? __ldg(view.at(boff + k)) : 0u;
+                const uint32_t y = valid ? view.vid(__ldg(view.at(boff + k))) : 0u;
                 cnt.hits += op.edge(valid && y != kTomb, bx, bp, y);
             }
         }
@@ -167,7 +171,7 @@ __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint3
         const uint32_t wdeg = __shfl_sync(kFull, deg, leader);
         const uint64_t woff = __shfl_sync(kFull, static_cast<unsigned long long>(off), leader);
         if (lane == leader) med = false;
-        sweep_row<32u>(view.at(woff), wdeg, lane, wx, wp, op, cnt);
+        sweep_row<32u>(view, view.at(woff), wdeg, lane, wx, wp, op, cnt);
     }
 
     // Tier 3: small rows gathered through a warp scan.
@@ -203,7 +207,7 @@ __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint3
             }
             ox = sm.f_x[wb + lo];
             op_ = sm.f_payload[wb + lo];
-            y = __ldg(sm.f_ptr[wb + lo] + (e - sm.f_scan[wb + lo]));
+            y = view.vid(__ldg(sm.f_ptr[wb + lo] + (e - sm.f_scan[wb + lo])));
         }
         cnt.hits += op.edge(valid && y != kTomb, ox, op_, y);
     }
@@ -227,7 +231,7 @@ __device__ __forceinline__ void expand_deferred(const AdjView &view, const BigRo
             // segment boundary: one pointer serves it.
             const uint32_t base = static_cast<uint32_t>(g - prefix) * kSplitChunk;
             const uint32_t len = min(kSplitChunk, r.deg - base);
-            sweep_row<TPB>(view.at(r.off + base), len, threadIdx.x, r.x, static_cast<P>(r.payload), op, cnt);
+            sweep_row<TPB>(view, view.at(r.off + base), len, threadIdx.x, r.x, static_cast<P>(r.payload), op, cnt);
         }
         prefix += chunks;
     }

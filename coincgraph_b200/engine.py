@@ -13,7 +13,9 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libcig.so")
+# CIG_LIBRARY selects another build of the engine (e.g. the bounds-checked
+# libcig_bc.so); the default is the release build next to this file.
+LIB_PATH = os.environ.get("CIG_LIBRARY") or os.path.join(_HERE, "libcig.so")
 
 BFS, SSSP, CC, PR = 0, 1, 2, 3
 ALGOS = {"bfs": BFS, "sssp": SSSP, "cc": CC, "pr": PR}
@@ -227,6 +229,7 @@ SIGNATURES = [
     ("cig_profile_read", _i32, [_vp, ctypes.POINTER(StageProfile), _u32]),
     ("cig_bfs_csr_noalloc", _i32, [_vp, _vp, _u32, _u32, _vp, _vp]),
     ("cig_memory_info_get", _i32, [_vp, ctypes.POINTER(MemoryInfo)]),
+    ("cig_build_info", _i32, [ctypes.POINTER(_i32), ctypes.POINTER(_i32)]),
     ("cig_apply_batches_device", _i32, [_vp, ctypes.POINTER(UpdateBatch), _u32, ctypes.POINTER(BatchStats), _vp]),
     ("cig_autotune", _i32, [_vp, ctypes.POINTER(TuneResult)]),
     ("cig_serve_start", _i32, [_vp, ctypes.POINTER(ServeOptions)]),
@@ -539,3 +542,12 @@ class Engine:
 
 def version() -> str:
     return load_library().cig_version().decode()
+
+
+def build_info() -> dict:
+    """{"binary_version": 100 for sm_100a, "bounds_checked": bool}; needs a GPU."""
+    bv, bc = ctypes.c_int(), ctypes.c_int()
+    rc = load_library().cig_build_info(ctypes.byref(bv), ctypes.byref(bc))
+    if rc != 0:
+        raise CigError(rc, load_library().cig_last_error(None).decode())
+    return {"binary_version": bv.value, "bounds_checked": bool(bc.value)}

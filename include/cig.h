@@ -378,6 +378,12 @@ int cig_bfs_csr_noalloc(const uint64_t *xadj, const uint32_t *adj, uint32_t n, u
 /* Library version string. */
 const char *cig_version(void);
 
+/* SASS architecture the engine's kernels were compiled for, as
+ * cudaFuncGetAttributes reports it on the current device (100 = sm_100a),
+ * and whether this is the bounds-checked build (libcig_bc.so).  No
+ * reference counterpart. */
+int cig_build_info(int *binary_version, int *bounds_checked);
+
 #ifdef __cplusplus
 }
 #endif

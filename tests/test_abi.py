@@ -18,7 +18,8 @@ def declared(header: str) -> list[str]:
     return sorted(set(names))
 
 
-@pytest.mark.parametrize("header,lib", [("cig.h", "libcig.so"), ("cig_gen.h", "libcig_gen.so")])
+@pytest.mark.parametrize("header,lib", [("cig.h", "libcig.so"), ("cig.h", "libcig_bc.so"),
+                                        ("cig_gen.h", "libcig_gen.so")])
 def test_library_exports_header(built, header, lib):
     path = os.path.join(ROOT, "coincgraph_b200", lib)
     so = ctypes.CDLL(path)
@@ -35,11 +36,20 @@ def test_binding_covers_header(built):
     assert set(declared("cig.h")) == bound
 
 
-def test_engine_library_targets_sm100a(built):
-    # the engine is a fat binary for sm_100a only; cuobjdump is not used (only
-    # the ELF section list is read through the loader's view of the file).
-    data = open(os.path.join(ROOT, "coincgraph_b200", "libcig.so"), "rb").read()
-    assert b".nv_fatbin" in data
+def test_engine_builds_for_sm100a_only(built):
+    # The compile lines name one target, sm_100a (the GPU tests confirm it
+    # through cig_build_info: binaryVersion 100).
+    from coincgraph_b200 import build
+
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def test_bounds_checked_library_reports_itself(built):
+    lib = ctypes.CDLL(os.path.join(ROOT, "coincgraph_b200", "libcig_bc.so"))
+    bc = ctypes.c_int(-1)
+    assert lib.cig_build_info(None, ctypes.byref(bc)) == 0 and bc.value == 1
+    rel = ctypes.CDLL(os.path.join(ROOT, "coincgraph_b200", "libcig.so"))
+    assert rel.cig_build_info(None, ctypes.byref(bc)) == 0 and bc.value == 0
 
 
 def test_options_defaults_match_reference_flags(built):
