@@ -199,6 +199,8 @@ enum SmallIdx : int {
     kCompactCountR = 24,
     kOrderedCountR = 25,
     kIndexedCountR = 26,
+    kCoopF = 27,  // addition groups left to mutate_add_warp, per arena
+    kCoopR = 28,
     kSmallCount = 32
 };
 
@@ -331,6 +333,7 @@ struct cig_handle {
     uint32_t *compact_r = nullptr, *chunks_r = nullptr, *chunk_end_r = nullptr, *ordered_r = nullptr;
     uint32_t *firstpos_r = nullptr, *indexed_groups_r = nullptr, *chunk_map_r = nullptr;
     uint8_t *gtype_r = nullptr;
+    uint32_t *coopf = nullptr, *coopr = nullptr;  // addition groups served one warp each
     void *cub_r = nullptr;
     size_t cub_r_bytes = 0;
     // flat deletion: per-group chunk counts, their inclusive prefix sum, the
@@ -956,6 +959,8 @@ struct cig_handle {
         dfree(firstpos_r);
         dfree(indexed_groups_r);
         dfree(gtype_r);
+        dfree(coopf);
+        dfree(coopr);
         if (cub_r) cudaFree(cub_r);
         cub_r = nullptr;
         dfree(gflags);
@@ -1005,6 +1010,8 @@ struct cig_handle {
         dmalloc(gtype_r, cap);
         dmalloc(indexed_groups_r, cap);
         dmalloc(firstpos_r, cap);
+        dmalloc(coopf, cap);
+        dmalloc(coopr, cap);
         dmalloc(gflags, 4 * cap);
         dmalloc(gpos, 4 * cap);
         dmalloc(gendf, cap);
@@ -1695,9 +1702,17 @@ struct cig_handle {
         const int ps = prof_begin(CIG_STAGE_DEL_SCAN);
         launch(del_scan, sms * del_scan_blocks_per_sm(), kMutWarps * 32, A.view(), A.desc, sorted, grp, chunk_end,
                chunk_map, m, firstpos, status->counters, forward ? seg_hot : nullptr);
-        if (ix.keys)
+        if (ix.keys) {
+            // groups of more than kLaneKeys keys: one warp each (del_index_wide),
+            // listed in the arena's warp-group list (free during deletions)
+            uint32_t *wide = forward ? coopf : coopr;
+            uint32_t *wcount = small + (forward ? kCoopF : kCoopR);
+            CK(cudaMemsetAsync(wcount, 0, sizeof(uint32_t), cs));
             launch(del_index, persistent_grid(), 256, A.view(), A.desc, sorted, grp, indexed_groups, icount, firstpos,
-                   ix, stats, status);
+                   ix, wide, wcount, stats, status);
+            launch(del_index_wide, persistent_grid(), 256, A.view(), A.desc, sorted, grp, wide, wcount, firstpos, ix,
+                   stats, status);
+        }
         prof_end(ps);
         launch(del_apply, grid_for(nd), 256, A.view(), A.desc, sorted, m, firstpos, stats);
         launch(del_finish, persistent_grid(), 256, A.desc, sorted, grp, gtype, firstpos, compact, ccount, stats);
@@ -1747,8 +1762,13 @@ struct cig_handle {
         unsigned long long *stats = with_stats ? status->counters : nullptr;
         const uint32_t *vals = forward ? d_av : d_au;
         const PosIndex ix = pos_index(forward);
-        launch(mutate_add, persistent_grid(), 256, A.view(), A.desc, sorted, grp, plan, A.alloc, vals, big, bcount,
+        uint32_t *coop = forward ? coopf : coopr;
+        uint32_t *ccount = small + (forward ? kCoopF : kCoopR);
+        CK(cudaMemsetAsync(ccount, 0, sizeof(uint32_t), cs));
+        launch(mutate_add, persistent_grid(), 256, A.view(), A.desc, sorted, grp, plan, A.alloc, vals, coop, ccount,
                stats, ix, status);
+        launch(mutate_add_warp, persistent_grid(), 256, A.view(), A.desc, sorted, grp, plan, A.alloc, vals, coop,
+               ccount, big, bcount, stats, ix, status);
         launch(mutate_add_big, sms * 2, kTpbMut, A.view(), A.desc, sorted, grp, plan, A.alloc, vals, big, bcount,
                stats, ix, status);
         prof_end(p);
@@ -2747,9 +2767,11 @@ struct cig_handle {
         // Per slot of ensure_batch: 4 update arrays (4 B), 6 key/plan arrays
         // (8 B), 12 group/match/chunk arrays (4 B), `touched` (2 x 4 B), the
         // group type (1 B), flags + positions (2 x 4 x 4 B), group ends (2 x
-        // 4 B), packed whole-batch keys (2 x 4 x 8 B), addition groups (4 x 4 B).
-        const uint64_t per_slot = 16 + 48 + 48 + 8 + 1 + 32 + 8 + 64 + 16;
-        m->batch_buffers = bcap * per_slot + cub_bytes + chunk_map_cap * sizeof(uint32_t) +
+        // 4 B), packed whole-batch keys (2 x 4 x 8 B), addition groups (4 x 4 B),
+        // warp-served addition groups (2 x 4 B), the reverse arena's deletion
+        // scratch (6 x 4 B + 1 B).
+        const uint64_t per_slot = 16 + 48 + 48 + 8 + 1 + 32 + 8 + 64 + 16 + 8 + 6 * 4 + 1;
+        m->batch_buffers = bcap * per_slot + cub_bytes + cub_r_bytes + 2 * chunk_map_cap * sizeof(uint32_t) +
                            (opt.algo == CIG_PR ? 2 * bcap * sizeof(double) : 0) +
                            static_cast<uint64_t>(bsnap_cap) * 41 * sizeof(unsigned long long);
         if (qstream)

@@ -640,16 +640,16 @@ __device__ __forceinline__ uint32_t del_index_key(const AdjView &view, RowDesc *
 
 __global__ void del_index(AdjView view, RowDesc *desc, const unsigned long long *keys, Groups gr,
                           const uint32_t *list, const uint32_t *count, uint32_t *firstpos, PosIndex ix,
-                          unsigned long long *stats, Status *st) {
+                          uint32_t *wide, uint32_t *wide_count, unsigned long long *stats, Status *st) {
     const uint32_t lane = lane_id();
     uint32_t removed = 0;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t nl = *count;
     for (uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; base < nl; base += warps * 32u) {
         const uint32_t i = base + lane;
-        uint32_t gs = 0, nk = 0;
+        uint32_t g = 0, gs = 0, nk = 0;
         if (i < nl) {
-            const uint32_t g = list[i];
+            g = list[i];
             gs = gr.start[g];
             nk = gr.end[g] - gs;
         }
@@ -659,17 +659,31 @@ __global__ void del_index(AdjView view, RowDesc *desc, const unsigned long long 
             for (uint32_t j = 0; j < nk; ++j)
                 removed += del_index_key(view, desc, d, u, key_low(keys[gs + j]), firstpos + gs + j, ix, st);
         }
-        uint32_t todo = __ballot_sync(kFull, i < nl && nk > kLaneKeys);
-        while (todo) {
-            const int b = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const uint32_t bs = __shfl_sync(kFull, gs, b);
-            const uint32_t bk = __shfl_sync(kFull, nk, b);
-            const uint32_t u = key_src(keys[bs]);
-            const RowDesc d = desc[u];
-            for (uint32_t j = lane; j < bk; j += 32u)
-                removed += del_index_key(view, desc, d, u, key_low(keys[bs + j]), firstpos + bs + j, ix, st);
-        }
+        // Larger groups (hub rows) go to del_index_wide, one warp per group
+        // over the whole grid.
+        warp_enqueue(i < nl && nk > kLaneKeys, g, wide, wide_count, nl, st);
+    }
+    if (stats) warp_count(&stats[kCntRemoved], removed);
+}
+
+// The groups of more than kLaneKeys keys, one warp per group, lanes over the
+// keys (distinct keys of one row are independent: each has its own index
+// entry and position).
+__global__ void del_index_wide(AdjView view, RowDesc *desc, const unsigned long long *keys, Groups gr,
+                               const uint32_t *wide, const uint32_t *wide_count, uint32_t *firstpos, PosIndex ix,
+                               unsigned long long *stats, Status *st) {
+    const uint32_t lane = lane_id();
+    uint32_t removed = 0;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t nw = *wide_count;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nw; i += warps) {
+        const uint32_t g = wide[i];
+        const uint32_t gs = gr.start[g];
+        const uint32_t nk = gr.end[g] - gs;
+        const uint32_t u = key_src(keys[gs]);
+        const RowDesc d = desc[u];
+        for (uint32_t j = lane; j < nk; j += 32u)
+            removed += del_index_key(view, desc, d, u, key_low(keys[gs + j]), firstpos + gs + j, ix, st);
     }
     if (stats) warp_count(&stats[kCntRemoved], removed);
 }
@@ -1057,21 +1071,24 @@ __global__ void alloc_classes(ArenaAlloc *al, Status *st) {
     }
 }
 
-// Addition phase.  A warp takes 32 groups: each lane serves its own group
-// alone when it is small (at most kLaneAdds appends, and a moving row of at
+// Addition phase.  mutate_add gives each lane a group of its own when the
+// lane can serve it alone (at most kLaneAdds appends, and a moving row of at
 // most kLaneRow slots, read into registers with independent loads: rows in
 // host memory cost one round trip, not one per entry), so the common
-// one-request groups run 32 to a warp;
-// the other groups are then served one at a time by the whole warp (rows
-// above kWarpRowMax that must move go to the block path).  `vals` is add_v
-// for the forward arena and add_u for the reverse arena.  A moving row is
-// copied without its tombstones.
+// one-request groups run 32 to a warp.  The other groups are appended to a
+// list that mutate_add_warp serves one warp per group over the whole grid
+// (rows above kWarpRowMax that must move go on to the block path,
+// mutate_add_big).  Serving them inside the warp that found them left the
+// busiest warps a serial queue of up to 32 row copies while most of the grid
+// had no group at all.  `vals` is add_v for the forward arena and add_u for
+// the reverse arena.  A moving row is copied without its tombstones.
 constexpr uint32_t kLaneAdds = 8;
 constexpr uint32_t kLaneRow = 8;
 
 __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long *keys, Groups gr,
-                           const unsigned long long *plan, const ArenaAlloc *al, const uint32_t *vals, uint32_t *big,
-                           uint32_t *big_count, unsigned long long *stats, PosIndex ix, Status *st) {
+                           const unsigned long long *plan, const ArenaAlloc *al, const uint32_t *vals,
+                           uint32_t *coop_list, uint32_t *coop_count, unsigned long long *stats, PosIndex ix,
+                           Status *st) {
     if (ld_volatile(&st->err) & kErrArena) return;
     const uint32_t lane = lane_id();
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -1125,81 +1142,102 @@ __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long
                 }
             }
         }
-        uint32_t todo = __ballot_sync(kFull, coop);
-        while (todo) {
-            const int bl = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const uint32_t gb = base + static_cast<uint32_t>(bl);
-            const unsigned long long p = plan[gb];
-            const uint32_t gs = gr.start[gb];
-            const uint32_t ge = gr.end[gb];
-            const uint32_t u = key_src(keys[gs]);
-            const RowDesc d = desc[u];
-            const uint32_t a = ge - gs;
-            if (p == kKeyNone) {
-                const bool indexed = idx_row(ix, u);
-                for (uint32_t j = lane; j < a; j += 32u) {
-                    const uint32_t v = vals[key_low(keys[gs + j])];
-                    write_slot(view, d.off + d.len + j, v);
-                    if (indexed) idx_add(ix, u, v, d.len + j, st);
-                }
-                if (lane == 0) desc[u] = RowDesc{d.off, d.len + a, d.meta};
-            } else {
-                if (d.len > kWarpRowMax) {
-                    if (lane == 0) big[atomicAdd(big_count, 1u)] = gb;
-                    continue;
-                }
-                const uint32_t cls = static_cast<uint32_t>(p >> 32);
-                const unsigned long long off = alloc_offset(al, cls, static_cast<uint32_t>(p));
-                // Copy the survivors in order, 256 entries per step: each lane
-                // issues two independent 16-byte loads (the old block lies in
-                // one segment and starts on a 16-byte boundary) before any
-                // store, so a zero-copy row costs one host round trip per
-                // 256 entries instead of one per 32.
-                const uint32_t *src = view.at(d.off);
-                uint32_t w = 0;
-                for (uint32_t b0 = 0; b0 < d.len; b0 += 256u) {
-                    uint32_t e[8];
-#pragma unroll
-                    for (uint32_t h = 0; h < 2; ++h) {
-                        const uint32_t k = b0 + 128u * h + 4u * lane;
-                        uint4 q = make_uint4(kTomb, kTomb, kTomb, kTomb);
-                        if (k < d.len) q = *reinterpret_cast<const uint4 *>(src + k);
-                        e[4 * h] = k < d.len ? q.x : kTomb;
-                        e[4 * h + 1] = k + 1u < d.len ? q.y : kTomb;
-                        e[4 * h + 2] = k + 2u < d.len ? q.z : kTomb;
-                        e[4 * h + 3] = k + 3u < d.len ? q.w : kTomb;
-                    }
-#pragma unroll
-                    for (uint32_t h = 0; h < 2; ++h) {
-                        uint32_t c = 0;
-#pragma unroll
-                        for (uint32_t j = 0; j < 4; ++j) c += e[4 * h + j] != kTomb ? 1u : 0u;
-                        uint32_t incl = c;
-#pragma unroll
-                        for (uint32_t o = 1; o < 32u; o <<= 1) {
-                            const uint32_t t = __shfl_up_sync(kFull, incl, o);
-                            if (lane >= o) incl += t;
-                        }
-                        uint32_t pos = w + incl - c;
-#pragma unroll
-                        for (uint32_t j = 0; j < 4; ++j)
-                            if (e[4 * h + j] != kTomb) write_slot(view, off + pos++, e[4 * h + j]);
-                        w += __shfl_sync(kFull, incl, 31);
-                    }
-                }
-                if (lane == 0) moved_entries += w;
-                for (uint32_t j = lane; j < a; j += 32u) write_slot(view, off + w + j, vals[key_low(keys[gs + j])]);
-                if (lane == 0) desc[u] = RowDesc{off, w + a, rd_meta(cls, 0)};
-                if (idx_row(ix, u)) {
-                    // survivors moved: reposition them; then count the appended entries
-                    idx_reposition_warp(view, ix, u, off, w, st);
-                    for (uint32_t j = lane; j < a; j += 32u) idx_add(ix, u, vals[key_low(keys[gs + j])], w + j, st);
-                }
-                if (lane == 0) moved += 1;
+        // Groups a lane cannot serve alone go to the warp-per-group kernel,
+        // which spreads them over every warp of the grid.
+        warp_enqueue(coop, g, coop_list, coop_count, ng, st);
+    }
+    if (stats) {
+        warp_count(&stats[kCntChanged], changed);
+        warp_count(&stats[kCntRelocated], moved);
+        warp_count(&stats[kCntMovedEntries], moved_entries);
+    }
+}
+
+
+// The groups mutate_add left to whole warps (more than kLaneAdds appends, or
+// a moving row of more than kLaneRow entries), one warp per group over the
+// whole grid: rows of up to kWarpRowMax entries move here, larger ones go to
+// mutate_add_big.
+__global__ void mutate_add_warp(AdjView view, RowDesc *desc, const unsigned long long *keys, Groups gr,
+                                const unsigned long long *plan, const ArenaAlloc *al, const uint32_t *vals,
+                                const uint32_t *coop_list, const uint32_t *coop_count, uint32_t *big,
+                                uint32_t *big_count, unsigned long long *stats, PosIndex ix, Status *st) {
+    if (ld_volatile(&st->err) & kErrArena) return;
+    const uint32_t lane = lane_id();
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t nc = *coop_count;
+    uint32_t changed = 0, moved = 0, moved_entries = 0;  // lane 0 counts
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nc; i += warps) {
+        const uint32_t gb = coop_list[i];
+        const unsigned long long p = plan[gb];
+        const uint32_t gs = gr.start[gb];
+        const uint32_t ge = gr.end[gb];
+        const uint32_t u = key_src(keys[gs]);
+        const RowDesc d = desc[u];
+        const uint32_t a = ge - gs;
+        if (p == kKeyNone) {
+            const bool indexed = idx_row(ix, u);
+            for (uint32_t j = lane; j < a; j += 32u) {
+                const uint32_t v = vals[key_low(keys[gs + j])];
+                write_slot(view, d.off + d.len + j, v);
+                if (indexed) idx_add(ix, u, v, d.len + j, st);
             }
-            if (lane == 0) changed += 1;
+            if (lane == 0) desc[u] = RowDesc{d.off, d.len + a, d.meta};
+        } else {
+            if (d.len > kWarpRowMax) {
+                if (lane == 0) big[atomicAdd(big_count, 1u)] = gb;
+                continue;
+            }
+            const uint32_t cls = static_cast<uint32_t>(p >> 32);
+            const unsigned long long off = alloc_offset(al, cls, static_cast<uint32_t>(p));
+            // Copy the survivors in order, 256 entries per step: each lane
+            // issues two independent 16-byte loads (the old block lies in
+            // one segment and starts on a 16-byte boundary) before any
+            // store, so a zero-copy row costs one host round trip per
+            // 256 entries instead of one per 32.
+            const uint32_t *src = view.at(d.off);
+            uint32_t w = 0;
+            for (uint32_t b0 = 0; b0 < d.len; b0 += 256u) {
+                uint32_t e[8];
+#pragma unroll
+                for (uint32_t h = 0; h < 2; ++h) {
+                    const uint32_t k = b0 + 128u * h + 4u * lane;
+                    uint4 q = make_uint4(kTomb, kTomb, kTomb, kTomb);
+                    if (k < d.len) q = *reinterpret_cast<const uint4 *>(src + k);
+                    e[4 * h] = k < d.len ? q.x : kTomb;
+                    e[4 * h + 1] = k + 1u < d.len ? q.y : kTomb;
+                    e[4 * h + 2] = k + 2u < d.len ? q.z : kTomb;
+                    e[4 * h + 3] = k + 3u < d.len ? q.w : kTomb;
+                }
+#pragma unroll
+                for (uint32_t h = 0; h < 2; ++h) {
+                    uint32_t c = 0;
+#pragma unroll
+                    for (uint32_t j = 0; j < 4; ++j) c += e[4 * h + j] != kTomb ? 1u : 0u;
+                    uint32_t incl = c;
+#pragma unroll
+                    for (uint32_t o = 1; o < 32u; o <<= 1) {
+                        const uint32_t t = __shfl_up_sync(kFull, incl, o);
+                        if (lane >= o) incl += t;
+                    }
+                    uint32_t pos = w + incl - c;
+#pragma unroll
+                    for (uint32_t j = 0; j < 4; ++j)
+                        if (e[4 * h + j] != kTomb) write_slot(view, off + pos++, e[4 * h + j]);
+                    w += __shfl_sync(kFull, incl, 31);
+                }
+            }
+            if (lane == 0) moved_entries += w;
+            for (uint32_t j = lane; j < a; j += 32u) write_slot(view, off + w + j, vals[key_low(keys[gs + j])]);
+            if (lane == 0) desc[u] = RowDesc{off, w + a, rd_meta(cls, 0)};
+            if (idx_row(ix, u)) {
+                // survivors moved: reposition them; then count the appended entries
+                idx_reposition_warp(view, ix, u, off, w, st);
+                for (uint32_t j = lane; j < a; j += 32u) idx_add(ix, u, vals[key_low(keys[gs + j])], w + j, st);
+            }
+            if (lane == 0) moved += 1;
         }
+        if (lane == 0) changed += 1;
     }
     if (stats) {
         warp_count(&stats[kCntChanged], changed);
