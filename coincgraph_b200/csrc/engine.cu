@@ -201,6 +201,8 @@ enum SmallIdx : int {
     kIndexedCountR = 26,
     kCoopF = 27,  // addition groups left to mutate_add_warp, per arena
     kCoopR = 28,
+    kHugeF = 29,  // hub deletion groups served by the whole grid, per arena
+    kHugeR = 30,
     kSmallCount = 32
 };
 
@@ -334,6 +336,7 @@ struct cig_handle {
     uint32_t *firstpos_r = nullptr, *indexed_groups_r = nullptr, *chunk_map_r = nullptr;
     uint8_t *gtype_r = nullptr;
     uint32_t *coopf = nullptr, *coopr = nullptr;  // addition groups served one warp each
+    uint32_t *hugef = nullptr, *huger = nullptr;  // hub deletion groups served by the grid
     void *cub_r = nullptr;
     size_t cub_r_bytes = 0;
     // flat deletion: per-group chunk counts, their inclusive prefix sum, the
@@ -961,6 +964,8 @@ struct cig_handle {
         dfree(gtype_r);
         dfree(coopf);
         dfree(coopr);
+        dfree(hugef);
+        dfree(huger);
         if (cub_r) cudaFree(cub_r);
         cub_r = nullptr;
         dfree(gflags);
@@ -1012,6 +1017,8 @@ struct cig_handle {
         dmalloc(firstpos_r, cap);
         dmalloc(coopf, cap);
         dmalloc(coopr, cap);
+        dmalloc(hugef, cap);
+        dmalloc(huger, cap);
         dmalloc(gflags, 4 * cap);
         dmalloc(gpos, 4 * cap);
         dmalloc(gendf, cap);
@@ -1703,15 +1710,19 @@ struct cig_handle {
         launch(del_scan, sms * del_scan_blocks_per_sm(), kMutWarps * 32, A.view(), A.desc, sorted, grp, chunk_end,
                chunk_map, m, firstpos, status->counters, forward ? seg_hot : nullptr);
         if (ix.keys) {
-            // groups of more than kLaneKeys keys: one warp each (del_index_wide),
-            // listed in the arena's warp-group list (free during deletions)
+            // groups of more than kLaneKeys keys: one warp each, hub groups the
+            // whole grid (del_index_wide); the warp list is the arena's
+            // addition warp-group list, free during deletions
             uint32_t *wide = forward ? coopf : coopr;
+            uint32_t *huge = forward ? hugef : huger;
             uint32_t *wcount = small + (forward ? kCoopF : kCoopR);
+            uint32_t *hcount = small + (forward ? kHugeF : kHugeR);
             CK(cudaMemsetAsync(wcount, 0, sizeof(uint32_t), cs));
+            CK(cudaMemsetAsync(hcount, 0, sizeof(uint32_t), cs));
             launch(del_index, persistent_grid(), 256, A.view(), A.desc, sorted, grp, indexed_groups, icount, firstpos,
-                   ix, wide, wcount, stats, status);
-            launch(del_index_wide, persistent_grid(), 256, A.view(), A.desc, sorted, grp, wide, wcount, firstpos, ix,
-                   stats, status);
+                   ix, wide, wcount, huge, hcount, stats, status);
+            launch(del_index_wide, persistent_grid(), 256, A.view(), A.desc, sorted, grp, wide, wcount, huge, hcount,
+                   firstpos, ix, stats, status);
         }
         prof_end(ps);
         launch(del_apply, grid_for(nd), 256, A.view(), A.desc, sorted, m, firstpos, stats);
@@ -2768,9 +2779,9 @@ struct cig_handle {
         // (8 B), 12 group/match/chunk arrays (4 B), `touched` (2 x 4 B), the
         // group type (1 B), flags + positions (2 x 4 x 4 B), group ends (2 x
         // 4 B), packed whole-batch keys (2 x 4 x 8 B), addition groups (4 x 4 B),
-        // warp-served addition groups (2 x 4 B), the reverse arena's deletion
+        // warp-served addition and hub deletion groups (4 x 4 B), the reverse arena's deletion
         // scratch (6 x 4 B + 1 B).
-        const uint64_t per_slot = 16 + 48 + 48 + 8 + 1 + 32 + 8 + 64 + 16 + 8 + 6 * 4 + 1;
+        const uint64_t per_slot = 16 + 48 + 48 + 8 + 1 + 32 + 8 + 64 + 16 + 16 + 6 * 4 + 1;
         m->batch_buffers = bcap * per_slot + cub_bytes + cub_r_bytes + 2 * chunk_map_cap * sizeof(uint32_t) +
                            (opt.algo == CIG_PR ? 2 * bcap * sizeof(double) : 0) +
                            static_cast<uint64_t>(bsnap_cap) * 41 * sizeof(unsigned long long);

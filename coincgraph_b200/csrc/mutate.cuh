@@ -609,13 +609,18 @@ __global__ void del_classify(const RowDesc *desc, const unsigned long long *keys
 // to the next one (a scan from the deleted position on, rare: parallel
 // edges).  The tombstone is written here at once (the position is final),
 // and the position is recorded with kApplied set so that del_apply skips
-// it.  Most groups hold one or two keys, so each lane takes a group of up
-// to kLaneKeys keys alone; larger groups are served by the whole warp.
+// it.  A warp deals the keys of its groups of up to kLaneKeys keys one per
+// lane (del_index); larger groups get a warp each, and groups of more than
+// kHugeKeys keys the whole grid (del_index_wide).
 constexpr uint32_t kLaneKeys = 4;
+constexpr uint32_t kHugeKeys = 256;
 constexpr uint32_t kApplied = 0x80000000u;  // firstpos flag: tombstone already written
 
+// `count_tomb`: add the tombstone to the row's descriptor here (callers that
+// serve many keys of one row add their warp's total once instead).
 __device__ __forceinline__ uint32_t del_index_key(const AdjView &view, RowDesc *desc, const RowDesc &d, uint32_t u,
-                                                  uint32_t v, uint32_t *fp, const PosIndex &ix, Status *st) {
+                                                  uint32_t v, uint32_t *fp, const PosIndex &ix, Status *st,
+                                                  bool count_tomb = true) {
     const unsigned long long s = idx_find(ix, (static_cast<unsigned long long>(u) << 32) | v);
     if (s == ~0ull) return 0u;  // not in the row: a missing delete
     const uint2 e = ix.val[s];
@@ -625,7 +630,7 @@ __device__ __forceinline__ uint32_t del_index_key(const AdjView &view, RowDesc *
     }
     *fp = e.x | kApplied;
     write_slot(view, d.off + e.x, kTomb);
-    atomicAdd(&desc[u].meta, 1u << 6);
+    if (count_tomb) atomicAdd(&desc[u].meta, 1u << 6);
     if (e.y == 1u) {
         ix.val[s] = make_uint2(kInf, 0u);
         ix.keys[s] = kIdxDeleted;
@@ -640,7 +645,8 @@ __device__ __forceinline__ uint32_t del_index_key(const AdjView &view, RowDesc *
 
 __global__ void del_index(AdjView view, RowDesc *desc, const unsigned long long *keys, Groups gr,
                           const uint32_t *list, const uint32_t *count, uint32_t *firstpos, PosIndex ix,
-                          uint32_t *wide, uint32_t *wide_count, unsigned long long *stats, Status *st) {
+                          uint32_t *wide, uint32_t *wide_count, uint32_t *huge, uint32_t *huge_count,
+                          unsigned long long *stats, Status *st) {
     const uint32_t lane = lane_id();
     uint32_t removed = 0;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -653,37 +659,91 @@ __global__ void del_index(AdjView view, RowDesc *desc, const unsigned long long 
             gs = gr.start[g];
             nk = gr.end[g] - gs;
         }
-        if (i < nl && nk <= kLaneKeys) {
-            const uint32_t u = key_src(keys[gs]);
-            const RowDesc d = desc[u];
-            for (uint32_t j = 0; j < nk; ++j)
-                removed += del_index_key(view, desc, d, u, key_low(keys[gs + j]), firstpos + gs + j, ix, st);
+        // The warp's small groups (up to kLaneKeys keys) are concatenated (a
+        // warp scan of their sizes) and their keys dealt one per lane, at
+        // most kLaneKeys steps; distinct keys of a row are independent.
+        const bool small_g = i < nl && nk <= kLaneKeys;
+        const uint32_t mine = small_g ? nk : 0u;
+        uint32_t incl = mine;
+#pragma unroll
+        for (uint32_t o = 1; o < 32u; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += t;
         }
-        // Larger groups (hub rows) go to del_index_wide, one warp per group
-        // over the whole grid.
-        warp_enqueue(i < nl && nk > kLaneKeys, g, wide, wide_count, nl, st);
+        const uint32_t excl = incl - mine;
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        for (uint32_t e0 = 0; e0 < total; e0 += 32u) {
+            const uint32_t e = e0 + lane;
+            uint32_t lo = 0, hi = 32;  // the last lane whose keys start at or before e
+#pragma unroll
+            for (int step = 0; step < 5; ++step) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (__shfl_sync(kFull, excl, mid) <= e)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            const uint32_t ks = __shfl_sync(kFull, gs, lo) + (e - __shfl_sync(kFull, excl, lo));
+            if (e < total) {
+                const uint32_t u = key_src(keys[ks]);
+                removed += del_index_key(view, desc, desc[u], u, key_low(keys[ks]), firstpos + ks, ix, st);
+            }
+        }
+        // Larger groups go to del_index_wide: up to kHugeKeys keys one warp
+        // per group, more (hub rows, where uniform deletions over the edges
+        // concentrate) across the whole grid in 32-key chunks.
+        warp_enqueue(i < nl && nk > kLaneKeys && nk <= kHugeKeys, g, wide, wide_count, nl, st);
+        warp_enqueue(i < nl && nk > kHugeKeys, g, huge, huge_count, nl, st);
     }
     if (stats) warp_count(&stats[kCntRemoved], removed);
 }
 
-// The groups of more than kLaneKeys keys, one warp per group, lanes over the
-// keys (distinct keys of one row are independent: each has its own index
-// entry and position).
 __global__ void del_index_wide(AdjView view, RowDesc *desc, const unsigned long long *keys, Groups gr,
-                               const uint32_t *wide, const uint32_t *wide_count, uint32_t *firstpos, PosIndex ix,
+                               const uint32_t *wide, const uint32_t *wide_count, const uint32_t *huge,
+                               const uint32_t *huge_count, uint32_t *firstpos, PosIndex ix,
                                unsigned long long *stats, Status *st) {
     const uint32_t lane = lane_id();
     uint32_t removed = 0;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nw = *wide_count;
-    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nw; i += warps) {
+    for (uint32_t i = wid; i < nw; i += warps) {
         const uint32_t g = wide[i];
         const uint32_t gs = gr.start[g];
         const uint32_t nk = gr.end[g] - gs;
         const uint32_t u = key_src(keys[gs]);
         const RowDesc d = desc[u];
+        uint32_t tombs = 0;
         for (uint32_t j = lane; j < nk; j += 32u)
-            removed += del_index_key(view, desc, d, u, key_low(keys[gs + j]), firstpos + gs + j, ix, st);
+            tombs += del_index_key(view, desc, d, u, key_low(keys[gs + j]), firstpos + gs + j, ix, st, false);
+        tombs = __reduce_add_sync(kFull, tombs);
+        if (lane == 0 && tombs) atomicAdd(&desc[u].meta, tombs << 6);
+        removed += lane == 0 ? tombs : 0u;
+    }
+    // Huge groups: chunk c of the concatenated 32-key chunks goes to warp
+    // c mod warps; every warp walks the (short) list in the same order.
+    const uint32_t nh = *huge_count;
+    uint64_t prefix = 0;
+    for (uint32_t h = 0; h < nh; ++h) {
+        const uint32_t g = huge[h];
+        const uint32_t gs = gr.start[g];
+        const uint32_t nk = gr.end[g] - gs;
+        const uint64_t chunks = (nk + 31u) / 32u;
+        uint64_t c = prefix + (wid + warps - static_cast<uint32_t>(prefix % warps)) % warps;
+        if (c < prefix + chunks) {
+            const uint32_t u = key_src(keys[gs]);
+            const RowDesc d = desc[u];
+            uint32_t tombs = 0;
+            for (; c < prefix + chunks; c += warps) {
+                const uint32_t j = static_cast<uint32_t>(c - prefix) * 32u + lane;
+                if (j < nk)
+                    tombs += del_index_key(view, desc, d, u, key_low(keys[gs + j]), firstpos + gs + j, ix, st, false);
+            }
+            tombs = __reduce_add_sync(kFull, tombs);
+            if (lane == 0 && tombs) atomicAdd(&desc[u].meta, tombs << 6);
+            removed += lane == 0 ? tombs : 0u;
+        }
+        prefix += chunks;
     }
     if (stats) warp_count(&stats[kCntRemoved], removed);
 }
@@ -1109,12 +1169,24 @@ __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long
                 const uint32_t u = key_src(keys[gs]);
                 const RowDesc d = desc[u];
                 const bool indexed = idx_row(ix, u);
+                // The appended values first, with independent loads (the
+                // stores below could alias them as far as the compiler knows).
+                uint32_t add[kLaneAdds];
+#pragma unroll
+                for (uint32_t j = 0; j < kLaneAdds; ++j) add[j] = j < a ? vals[key_low(keys[gs + j])] : 0u;
                 if (p == kKeyNone) {
-                    for (uint32_t j = 0; j < a; ++j) {
-                        const uint32_t v = vals[key_low(keys[gs + j])];
-                        write_slot(view, d.off + d.len + j, v);
-                        if (indexed) idx_add(ix, u, v, d.len + j, st);
+                    // A block of at most one segment: one slot lookup for the
+                    // row's end, then plain stores.
+                    if (rd_cls(d) <= kSegShift) {
+                        uint32_t *wp = view.wptr(d.off + d.len);
+#pragma unroll
+                        for (uint32_t j = 0; j < kLaneAdds; ++j)
+                            if (j < a) wp[j] = add[j];
+                    } else {
+                        for (uint32_t j = 0; j < a; ++j) write_slot(view, d.off + d.len + j, add[j]);
                     }
+                    if (indexed)
+                        for (uint32_t j = 0; j < a; ++j) idx_add(ix, u, add[j], d.len + j, st);
                     desc[u] = RowDesc{d.off, d.len + a, d.meta};
                     changed += 1;
                 } else if (d.len > kLaneRow) {
@@ -1122,20 +1194,26 @@ __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long
                 } else {
                     const uint32_t cls = static_cast<uint32_t>(p >> 32);
                     const unsigned long long off = alloc_offset(al, cls, static_cast<uint32_t>(p));
+                    // Old block (<= kLaneRow slots) and new block (<= 16 slots)
+                    // each lie in one segment: one slot lookup apiece.
                     uint32_t row[kLaneRow];
+                    const uint32_t *src = d.len ? view.at(d.off) : nullptr;
 #pragma unroll
-                    for (uint32_t k = 0; k < kLaneRow; ++k) row[k] = k < d.len ? *view.at(d.off + k) : kTomb;
+                    for (uint32_t k = 0; k < kLaneRow; ++k) row[k] = k < d.len ? src[k] : kTomb;
+                    uint32_t *wp = view.wptr(off);
                     uint32_t w = 0;
 #pragma unroll
                     for (uint32_t k = 0; k < kLaneRow; ++k)
-                        if (row[k] != kTomb) write_slot(view, off + w++, row[k]);
-                    for (uint32_t j = 0; j < a; ++j) write_slot(view, off + w + j, vals[key_low(keys[gs + j])]);
+                        if (row[k] != kTomb) wp[w++] = row[k];
+#pragma unroll
+                    for (uint32_t j = 0; j < kLaneAdds; ++j)
+                        if (j < a) wp[w + j] = add[j];
                     desc[u] = RowDesc{off, w + a, rd_meta(cls, 0)};
                     moved_entries += w;
                     if (indexed) {
-                        for (uint32_t k = 0; k < w; ++k) idx_pos_reset(ix, u, __ldcg(view.at(off + k)), st);
-                        for (uint32_t k = 0; k < w; ++k) idx_pos_set(ix, u, __ldcg(view.at(off + k)), k);
-                        for (uint32_t j = 0; j < a; ++j) idx_add(ix, u, vals[key_low(keys[gs + j])], w + j, st);
+                        for (uint32_t k = 0; k < w; ++k) idx_pos_reset(ix, u, __ldcg(wp + k), st);
+                        for (uint32_t k = 0; k < w; ++k) idx_pos_set(ix, u, __ldcg(wp + k), k);
+                        for (uint32_t j = 0; j < a; ++j) idx_add(ix, u, add[j], w + j, st);
                     }
                     moved += 1;
                     changed += 1;
