@@ -719,6 +719,7 @@ def uneven_stream(args, local, max_size, count):
         eng.close()
         del eng
     same = res["plain"]["digests"] == res["batched"]["digests"]
+    per_batch = {form: [round(x, 3) for x in res[form]["batch_ms"]] for form in res}
     return {
         "workload": f"{args.algo.upper()} RMAT s{args.scale} ef{args.edge_factor}{' symmetric' if symmetric else ''}, "
                     f"{len(sizes)} batches log-uniform [1k, {max_size}] (half del, half ins), cache {args.cache} GiB",
@@ -726,7 +727,7 @@ def uneven_stream(args, local, max_size, count):
         "plain_batches_per_s": len(sizes) / res["plain"]["wall_s"],
         "ratio": res["plain"]["wall_s"] / res["batched"]["wall_s"], "digests_equal": same,
         "timing": "host wall clock of the whole stream, synchronised at both ends",
-        "sizes": sizes.tolist(),
+        "sizes": sizes.tolist(), "batch_device_ms": per_batch,
         "plain": {"wall_s": res["plain"]["wall_s"], "p50_ms": statistics.median(res["plain"]["batch_ms"]),
                   "p99_ms": float(np.percentile(res["plain"]["batch_ms"], 99)), "launches": res["plain"]["launches"]},
         "batched": {"wall_s": res["batched"]["wall_s"], "launches": res["batched"]["launches"],

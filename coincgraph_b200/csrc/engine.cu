@@ -844,6 +844,7 @@ struct cig_handle {
         if (const char *e = std::getenv("CIG_LOCAL_SWEEPS")) local_sweeps = static_cast<uint32_t>(std::max(0, std::atoi(e)));
         if (opt.flags & CIG_FLAG_NO_GRAPHS) use_graphs = false;
         if (const char *e = std::getenv("CIG_GRAPHS")) use_graphs = std::atoi(e) != 0;
+        if (const char *e = std::getenv("CIG_MERGE_PUSH")) merge_push = std::atoi(e) != 0;
         if (const char *e = std::getenv("CIG_POS_INDEX")) use_index = std::atoi(e) != 0;
         if (const char *e = std::getenv("CIG_POS_INDEX_CLS")) index_cls = static_cast<uint32_t>(std::atoi(e));
         if (const char *e = std::getenv("CIG_POS_INDEX_HEADROOM"))
@@ -1331,6 +1332,9 @@ struct cig_handle {
         prof_end(p);
     }
     uint32_t local_sweeps = 8;  // block-local hops per closure round (CIG_LOCAL_SWEEPS; 0 = off)
+    // Whole batches run one push closure (after the insertions) instead of
+    // one per phase (CIG_MERGE_PUSH=0: one per phase, as the per-phase calls).
+    bool merge_push = true;
     uint32_t cc_shift = 0;      // CC: depth bits below the label in a value (also in Status)
     uint32_t *inval_done = nullptr;  // n + 1: vertices the invalidation sweeps expanded
 
@@ -1821,8 +1825,15 @@ struct cig_handle {
         ~InBatch() { flag = false; }
     };
 
+    // `push` false: leave the re-propagation from the repaired vertices to
+    // the insertion phase's push closure (whole batches, merge_push): their
+    // frontier stays queued and the insertion seeds join it, so one closure
+    // converges to the final graph's values.  The values after a whole batch
+    // are the unique fixpoint of the final graph either way; only the
+    // intermediate deletion-phase values, which a whole batch does not
+    // expose, are skipped.
     template <int A>
-    void delete_phase_dev(const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd) {
+    void delete_phase_dev(const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd, bool push = true) {
         const InBatch ib(in_batch);
         const uint32_t *ep = small + kEpoch;
         launch(phase_begin, 1, 32, small + kEpoch, small + kFr, 6u);  // frontier + affected counters
@@ -1849,13 +1860,14 @@ struct cig_handle {
         launch(enqueue_affected<A>, persistent_grid(), 256, list, small + kAffTotal, state, frontier(), status);
         prof_end(p);
         check_launch();
-        run_push<A>();
+        if (push) run_push<A>();
     }
 
+    // `fresh` false: keep the frontier the deletion phase left queued.
     template <int A>
-    void insert_phase_dev(const uint32_t *d_au, const uint32_t *d_av, uint64_t na) {
+    void insert_phase_dev(const uint32_t *d_au, const uint32_t *d_av, uint64_t na, bool fresh = true) {
         const InBatch ib(in_batch);
-        CK(cudaMemsetAsync(small + kFr, 0, 3 * sizeof(uint32_t), stream));
+        if (fresh) CK(cudaMemsetAsync(small + kFr, 0, 3 * sizeof(uint32_t), stream));
         fork_arenas([&] { mutate_add_arena(fwd, d_au, d_av, na, true, true); },
                     [&] { mutate_add_arena(rev, d_au, d_av, na, false, false); });
         int p = prof_begin(CIG_STAGE_SEED);
@@ -2022,9 +2034,9 @@ struct cig_handle {
                 constexpr int A = decltype(tag)::value;
                 presort_batch(d_du, d_dv, nd, d_au, d_av, na);
                 if (mutation_after) CK(cudaStreamWaitEvent(stream, mutation_after, 0));
-                delete_phase_dev<A>(d_du, d_dv, nd);
+                delete_phase_dev<A>(d_du, d_dv, nd, !merge_push);
                 CK(cudaEventRecord(e1, stream));
-                insert_phase_dev<A>(d_au, d_av, na);
+                insert_phase_dev<A>(d_au, d_av, na, !merge_push);
                 CK(cudaEventRecord(e2, stream));
                 presorted = false;
             });
@@ -2042,13 +2054,13 @@ struct cig_handle {
             bool sorted = false;
             run_graphed(3, nd, na, [&] {
                 sorted = presort_batch(du, dv, nd, au, av, na);
-                delete_phase_dev<A>(du, dv, nd);
+                delete_phase_dev<A>(du, dv, nd, !merge_push);
             });
             // A replay runs no host code: the whole-batch sort's outcome is
             // a function of the shape.
             presorted = sorted || presort_fits(nd, na);
             CK(cudaEventRecord(e1, stream));
-            run_graphed(4, nd, na, [&] { insert_phase_dev<A>(au, av, na); });
+            run_graphed(4, nd, na, [&] { insert_phase_dev<A>(au, av, na, !merge_push); });
             presorted = false;
             CK(cudaEventRecord(e2, stream));
         });

@@ -372,3 +372,24 @@ def test_cc_saturated_depths(bits, monkeypatch):
     run_case(adversarial_case(), "cc", CACHES["resident"])
     run_case(grid_case(24, 3, 80), "cc", CACHES["resident"])
     run_case_whole_batches(rmat_case(10, 3, 200, 200, seed_offset=21, symmetric=True), "cc", CACHES["mixed"])
+
+
+@pytest.mark.parametrize("algo", ["bfs", "sssp", "cc"])
+def test_whole_batch_single_push_closure(algo, monkeypatch):
+    """Whole batches run one push closure after the insertions (the repaired
+    vertices' frontier joins the insertion seeds); the values, rows and
+    parent witnesses equal the oracle's and those of one push per phase
+    (CIG_MERGE_PUSH=0) after every batch."""
+    case = rmat_case(11, 4, 300, 300, seed_offset=23)
+    out = {}
+    for merged in ("1", "0"):
+        monkeypatch.setenv("CIG_MERGE_PUSH", merged)
+        run_case_whole_batches(case, algo, CACHES["mixed"])
+        with make_engine(algo, cache_gib=4.0) as eng:
+            eng.load_csr(case.n, case.xadj, case.adj)
+            eng.init()
+            out[merged] = []
+            for b in case.batches:
+                eng.apply_batch(*b)
+                out[merged].append(eng.digest())
+    assert out["1"] == out["0"]
