@@ -1049,6 +1049,10 @@ struct cig_handle {
         CK(cudaHostAlloc(reinterpret_cast<void **>(&stage), 4 * cap * sizeof(uint32_t), cudaHostAllocDefault));
         bcap = cap;
         retire_graphs();
+        // Size the scan-chunk maps for the whole capacity now: a map that
+        // grew between the batches of a batched call synchronised in the
+        // middle of its queue.
+        if (fwd.seg_total) reserve_chunk_map(cap);
     }
 
     int key_end_bit() const {
