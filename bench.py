@@ -250,8 +250,10 @@ STAGE_KERNELS = {
 # multi-pass capture): profiles/<kernel>_*.md give the commands.  The
 # bench scales the ratio by this run's algorithmic bytes, an estimate.
 TRAFFIC_RATIO = {
-    "push_closure": (7.2, "ncu capture of push_closure, SSSP R-MAT s22 cache 4 GiB, 100k+100k batch "
-                          "(profiles/push_closure_sssp_s22_resident.md)"),
+    "push_closure": (5.97, "ncu capture of push_closure, SSSP R-MAT s22 cache 4 GiB, 100k+100k batch, "
+                           "10.3 MB DRAM against 1.73 MB algorithmic (profiles/closures_sssp_s22_cache4g.md)"),
+    "inval_closure": (6.09, "ncu capture of inval_closure, SSSP R-MAT s22 cache 4 GiB, 100k+100k batch, "
+                            "14.5 MB DRAM against 2.38 MB algorithmic (profiles/closures_sssp_s22_cache4g.md)"),
 }
 
 
@@ -523,15 +525,13 @@ def run_ours(args):
     link_peak = link_peak_gbs(torch, dev)
     stages = {n: stage_roofline(n, prof[n], hbm_peak, link_peak, nprof) for n in STAGE_KERNELS}
     stages = {n: v for n, v in stages.items() if v}
-    # The dominant kernel: among the stages that one kernel makes up (push:
-    # push_closure; inval: inval_closure; add: mostly mutate_add; del_scan:
-    # del_scan + del_index; pull: mostly pull_repair) the one with the most
-    # time.  (mutate, mutate_rev, group and cache are chains of 5-10 kernels
-    # each, and mutate/mutate_rev contain del_scan.)
-    dominant = max((n for n in ("push", "inval", "add", "del_scan", "pull") if n in stages),
-                   key=lambda n: stages[n]["ms_per_batch"])
-    main_kernel = {"push": "push_closure", "inval": "inval_closure", "add": "mutate_add", "del_scan": "del_scan",
-                   "pull": "pull_repair"}[dominant]
+    # The dominant kernel: of the stages that are one kernel each (push:
+    # push_closure, inval: inval_closure), the one with the most time; they
+    # are also the top two single-launch kernels of the ncu launch list
+    # (profiles/launches_sssp_s24_cache1g.md).  The other stages are chains
+    # of 2-10 kernels, and those of the two arenas overlap on two streams.
+    dominant = max((n for n in ("push", "inval") if n in stages), key=lambda n: stages[n]["ms_per_batch"])
+    main_kernel = {"push": "push_closure", "inval": "inval_closure"}[dominant]
     rf = stages[dominant]
     hbm_launch = rf["hbm_bytes_per_batch"] * nprof / max(prof[dominant]["launches"], 1)
     ratio = TRAFFIC_RATIO.get(main_kernel)
@@ -570,6 +570,10 @@ def run_ours(args):
             extra["served"] = served_stream(args, local, requests=args.served_requests, rate=args.served_rate)
         except Exception as e:
             extra["served"] = {"error": str(e)}
+        try:  # capacity: every request queued at once
+            extra["served_saturated"] = served_stream(args, local, requests=args.served_requests, rate=0.0)
+        except Exception as e:
+            extra["served_saturated"] = {"error": str(e)}
 
     if rank == 0:
         cpu = None
