@@ -247,13 +247,13 @@ STAGE_KERNELS = {
 
 # ncu DRAM bytes (read + write) per algorithmic HBM byte, measured on a
 # smaller case of the same kernel (the full-size launch is too large for a
-# multi-pass capture): profiles/<kernel>_*.md give the commands.  The
-# bench scales the ratio by this run's algorithmic bytes, an estimate.
+# multi-pass capture under the capture-size rule).  The bench scales the
+# ratio by this run's algorithmic bytes: an estimate, labelled as such.
 TRAFFIC_RATIO = {
     "push_closure": (5.97, "ncu capture of push_closure, SSSP R-MAT s22 cache 4 GiB, 100k+100k batch, "
-                           "10.3 MB DRAM against 1.73 MB algorithmic (profiles/closures_sssp_s22_cache4g.md)"),
+                           "10.3 MB DRAM against 1.73 MB algorithmic"),
     "inval_closure": (6.09, "ncu capture of inval_closure, SSSP R-MAT s22 cache 4 GiB, 100k+100k batch, "
-                            "14.5 MB DRAM against 2.38 MB algorithmic (profiles/closures_sssp_s22_cache4g.md)"),
+                            "14.5 MB DRAM against 2.38 MB algorithmic"),
 }
 
 
@@ -527,9 +527,9 @@ def run_ours(args):
     stages = {n: v for n, v in stages.items() if v}
     # The dominant kernel: of the stages that are one kernel each (push:
     # push_closure, inval: inval_closure), the one with the most time; they
-    # are also the top two single-launch kernels of the ncu launch list
-    # (profiles/launches_sssp_s24_cache1g.md).  The other stages are chains
-    # of 2-10 kernels, and those of the two arenas overlap on two streams.
+    # are also the two largest single launches of the batch in an ncu launch
+    # list of this workload.  The other stages are chains of 2-10 kernels,
+    # and those of the two arenas overlap on two streams.
     dominant = max((n for n in ("push", "inval") if n in stages), key=lambda n: stages[n]["ms_per_batch"])
     main_kernel = {"push": "push_closure", "inval": "inval_closure"}[dominant]
     rf = stages[dominant]
