@@ -1661,8 +1661,9 @@ struct cig_handle {
         prof[CIG_STAGE_GROUP].hits += 2 * na;
     }
 
+    // `zeroed`: the phase's counters were cleared by phase_begin.
     void mutate_delete_arena(DevArena &A, const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd, bool forward,
-                             bool with_stats) {
+                             bool with_stats, bool zeroed = false) {
         if (nd == 0) return;
         reserve_chunk_map(nd);  // before the map's address is taken below
         const uint32_t m = static_cast<uint32_t>(nd);
@@ -1695,23 +1696,22 @@ struct cig_handle {
             sorted = sort_keys(keys, tmp, nd);
             grp = build_groups(sorted, nd, groups, forward ? gendf : gendr, gcount);
         }
-        CK(cudaMemsetAsync(bcount, 0, sizeof(uint32_t), cs));
-        CK(cudaMemsetAsync(matched, 0, nd * sizeof(uint32_t), cs));
+        if (!zeroed) CK(cudaMemsetAsync(bcount, 0, sizeof(uint32_t), cs));
         prof_end(p);
         p = prof_begin(forward ? CIG_STAGE_MUTATE : CIG_STAGE_MUTATE_REV);
         unsigned long long *stats = with_stats ? status->counters : nullptr;
         uint32_t *ccount = small + (forward ? kCompactCount : kCompactCountR);
         uint32_t *ocount = small + (forward ? kOrderedCount : kOrderedCountR);
-        CK(cudaMemsetAsync(ccount, 0, sizeof(uint32_t), cs));
-        CK(cudaMemsetAsync(ocount, 0, sizeof(uint32_t), cs));
-        CK(cudaMemsetAsync(chunks, 0, nd * sizeof(uint32_t), cs));
-        CK(cudaMemsetAsync(firstpos, 0xFF, nd * sizeof(uint32_t), cs));
         // Flat path: rows whose deletion requests are all distinct.
         uint32_t *icount = small + (forward ? kIndexedCount : kIndexedCountR);
-        CK(cudaMemsetAsync(icount, 0, sizeof(uint32_t), cs));
+        if (!zeroed) {
+            CK(cudaMemsetAsync(ccount, 0, sizeof(uint32_t), cs));
+            CK(cudaMemsetAsync(ocount, 0, sizeof(uint32_t), cs));
+            CK(cudaMemsetAsync(icount, 0, sizeof(uint32_t), cs));
+        }
         const PosIndex ix = pos_index(forward);
         launch(del_classify, persistent_grid(), 256, A.desc, sorted, grp, chunks, gtype, ordered, ocount, ix,
-               indexed_groups, icount);
+               indexed_groups, icount, m, firstpos, matched);
         CK(cub::DeviceScan::InclusiveSum(scan_tmp, scan_tmp_bytes, chunks, chunk_end, static_cast<int>(nd), cs));
         launch(del_chunk_map, persistent_grid(), 256, grp, chunk_end, chunk_map);
         const int ps = prof_begin(CIG_STAGE_DEL_SCAN);
@@ -1725,8 +1725,10 @@ struct cig_handle {
             uint32_t *huge = forward ? hugef : huger;
             uint32_t *wcount = small + (forward ? kCoopF : kCoopR);
             uint32_t *hcount = small + (forward ? kHugeF : kHugeR);
-            CK(cudaMemsetAsync(wcount, 0, sizeof(uint32_t), cs));
-            CK(cudaMemsetAsync(hcount, 0, sizeof(uint32_t), cs));
+            if (!zeroed) {
+                CK(cudaMemsetAsync(wcount, 0, sizeof(uint32_t), cs));
+                CK(cudaMemsetAsync(hcount, 0, sizeof(uint32_t), cs));
+            }
             launch(del_index, persistent_grid(), 256, A.view(), A.desc, sorted, grp, indexed_groups, icount, firstpos,
                    ix, wide, wcount, huge, hcount, stats, status);
             launch(del_index_wide, persistent_grid(), 256, A.view(), A.desc, sorted, grp, wide, wcount, huge, hcount,
@@ -1840,17 +1842,22 @@ struct cig_handle {
     void delete_phase_dev(const uint32_t *d_du, const uint32_t *d_dv, uint64_t nd, bool push = true) {
         const InBatch ib(in_batch);
         const uint32_t *ep = small + kEpoch;
-        launch(phase_begin, 1, 32, small + kEpoch, small + kFr, 6u);  // frontier + affected counters
+        // frontier, affected and deletion-path counters of both arenas
+        static_assert(kSmallCount == 32 && kEpoch == 23, "phase_begin clears one 32-word counter block");
+        const uint32_t mask = (0x3Fu << kFr) | (1u << kBigF) | (1u << kBigR) | (1u << kCompactCount) |
+                              (1u << kOrderedCount) | (1u << kIndexedCount) | (1u << kInvalDone) |
+                              (1u << kCompactCountR) | (1u << kOrderedCountR) | (1u << kIndexedCountR) |
+                              (1u << kCoopF) | (1u << kCoopR) | (1u << kHugeF) | (1u << kHugeR);
+        launch(phase_begin, 1, 32, small + kEpoch, small, mask);
         int p = prof_begin(CIG_STAGE_SEED);
         if (nd)
             launch(seed_deletions<A>, grid_for(nd), 256, d_du, d_dv, static_cast<uint32_t>(nd), n, state,
                                                                 aff_stamp, ep, list, small + kAff, n + 1, status);
         prof_end(p);
         check_launch();
-        fork_arenas([&] { mutate_delete_arena(fwd, d_du, d_dv, nd, true, true); },
-                    [&] { mutate_delete_arena(rev, d_du, d_dv, nd, false, false); });
+        fork_arenas([&] { mutate_delete_arena(fwd, d_du, d_dv, nd, true, true, true); },
+                    [&] { mutate_delete_arena(rev, d_du, d_dv, nd, false, false, true); });
         p = prof_begin(CIG_STAGE_INVAL);
-        if (local_sweeps) CK(cudaMemsetAsync(small + kInvalDone, 0, sizeof(uint32_t), stream));
         launch_coop(inval_closure<A>, kTpb, fwd.view(), state, aff_stamp, ep, list, small + kAff, n + 1,
                     big_list(), n + 2, local_sweeps, inval_done, small + kInvalDone, small + kAffTotal, seg_hot,
                     status);

@@ -583,17 +583,45 @@ constexpr uint32_t kSmemKeys = 256;
 // when the row is indexed (posindex.cuh).
 enum : uint8_t { kGroupOrdered = 0, kGroupChunked = 1, kGroupIndexed = 2 };
 
+// Also clears the phase's per-key arrays (the scan chunk counts past the
+// groups, the first-match positions, the ordered path's match counts) for
+// the m keys, in place of three memsets.
 __global__ void del_classify(const RowDesc *desc, const unsigned long long *keys, Groups gr, uint32_t *chunks,
                              uint8_t *gtype, uint32_t *ordered, uint32_t *ordered_count, PosIndex ix,
-                             uint32_t *indexed, uint32_t *indexed_count) {
+                             uint32_t *indexed, uint32_t *indexed_count, uint32_t m, uint32_t *firstpos,
+                             uint32_t *matched) {
     const uint32_t ng = *gr.count;
     const uint32_t rounded = (ng + 31u) & ~31u;
+    const uint32_t lane = lane_id();
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        firstpos[i] = kInf;
+        matched[i] = 0u;
+        if (i >= ng) chunks[i] = 0u;
+    }
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < rounded; g += gridDim.x * blockDim.x) {
         bool dup = false, by_index = false;
+        uint32_t gs = 0, ge = 0;
         if (g < ng) {
-            const uint32_t gs = gr.start[g];
-            const uint32_t ge = gr.end[g];
-            for (uint32_t i = gs; i + 1 < ge && !dup; ++i) dup = keys[i] == keys[i + 1];
+            gs = gr.start[g];
+            ge = gr.end[g];
+            // Repeated requests are adjacent in the sorted keys; a lane checks
+            // its own group when it is short, the warp checks long ones (hub
+            // rows draw hundreds of deletions) together below.
+            if (ge - gs <= 32u)
+                for (uint32_t i = gs; i + 1 < ge && !dup; ++i) dup = keys[i] == keys[i + 1];
+        }
+        uint32_t longs = __ballot_sync(kFull, g < ng && ge - gs > 32u);
+        while (longs) {
+            const int l = __ffs(longs) - 1;
+            longs &= longs - 1;
+            const uint32_t ls = __shfl_sync(kFull, gs, l);
+            const uint32_t le = __shfl_sync(kFull, ge, l);
+            bool any = false;
+            for (uint32_t i = ls + lane; i + 1 < le; i += 32u) any |= keys[i] == keys[i + 1];
+            any = __any_sync(kFull, any);
+            if (lane == static_cast<uint32_t>(l)) dup = any;
+        }
+        if (g < ng) {
             const uint32_t u = key_src(keys[gs]);
             by_index = !dup && idx_row(ix, u);
             gtype[g] = dup ? kGroupOrdered : by_index ? kGroupIndexed : kGroupChunked;

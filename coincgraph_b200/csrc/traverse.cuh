@@ -525,10 +525,12 @@ __global__ void seed_deletions(const uint32_t *du, const uint32_t *dv, uint32_t 
 
 // Start of a deletion phase: advance the batch epoch (the "invalidated in
 // this batch" marker of aff_stamp, kept on the device so that a captured
-// batch graph needs no new arguments) and clear `count` counters.
-__global__ void phase_begin(uint32_t *epoch, uint32_t *counters, uint32_t count) {
+// batch graph needs no new arguments) and clear the counters of `counters`
+// (32 words) whose bit is set in `mask`, in place of one memset each.
+// Launched with 32 threads.
+__global__ void phase_begin(uint32_t *epoch, uint32_t *counters, uint32_t mask) {
     if (threadIdx.x == 0) *epoch += 1u;
-    if (threadIdx.x < count) counters[threadIdx.x] = 0u;
+    if (threadIdx.x < 32u && ((mask >> threadIdx.x) & 1u)) counters[threadIdx.x] = 0u;
 }
 
 // value <- initial value for every invalidated vertex (reset_affected_values,
