@@ -160,6 +160,9 @@ enum Counter : int {
     kCntMovedEntries = 34,
 };
 
+// Hint: bring the line holding `p` into L2 (no register result, no wait).
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;

@@ -1865,8 +1865,10 @@ struct cig_handle {
         p = prof_begin(CIG_STAGE_PULL);
         launch(reset_affected<A>, persistent_grid(), 256, list, small + kAffTotal, state, cc_shift);
         const BigList pull_big = big_list();
-        launch(pull_repair<A>, persistent_grid(), kTpb, rev.view(), state, aff_stamp, ep, list,
-                                                               small + kAffTotal, pull_big, status);
+        // One resident wave (__launch_bounds__(kTpb, 4)): a second wave of
+        // blocks would start its few rows only after the first wave ends.
+        launch(pull_repair<A>, sms * 4, kTpb, rev.view(), state, aff_stamp, ep, list, small + kAffTotal, pull_big,
+               status);
         launch(pull_deferred<A>, persistent_grid(), kTpb, rev.view(), state, aff_stamp, ep, pull_big, status);
         launch(enqueue_affected<A>, persistent_grid(), 256, list, small + kAffTotal, state, frontier(), status);
         prof_end(p);

@@ -15,6 +15,9 @@
 // appends.
 #pragma once
 
+#include <type_traits>
+#include <utility>
+
 #include "common.cuh"
 
 namespace cig {
@@ -72,32 +75,72 @@ struct Defer {
     uint32_t split;   // rows of at least this many entries are deferred
 };
 
+// Ops whose first access per edge is a plain load of a word of the edge's
+// target (its state word) expose it as `peek(y)` and take the loaded word in
+// `edge_peeked(valid, x, payload, y, word)`.  The sweeps then issue the loads
+// of a thread's entries together before any of them is used, instead of one
+// dependent load per edge() call.  Ops without peek() run edge() per entry.
+template <class Op, class = void>
+struct has_peek : std::false_type {};
+template <class Op>
+struct has_peek<Op, std::void_t<decltype(std::declval<const Op &>().peek(0u))>> : std::true_type {};
+
+// The four entries of a 16-byte row load: entry j is live when it lies
+// before `deg` (relative index k + j) and is not a tombstone.
+template <class Op, class P>
+__device__ __forceinline__ uint32_t edge4(const Op &op, uint4 q, uint32_t k, uint32_t deg, uint32_t x, P payload) {
+    const bool v0 = k < deg && q.x != kTomb, v1 = k + 1u < deg && q.y != kTomb;
+    const bool v2 = k + 2u < deg && q.z != kTomb, v3 = k + 3u < deg && q.w != kTomb;
+    uint32_t hits = 0;
+    if constexpr (has_peek<Op>::value) {
+        using W = decltype(op.peek(0u));
+        W w0{}, w1{}, w2{}, w3{};
+        if (v0) w0 = op.peek(q.x);
+        if (v1) w1 = op.peek(q.y);
+        if (v2) w2 = op.peek(q.z);
+        if (v3) w3 = op.peek(q.w);
+        hits += op.edge_peeked(v0, x, payload, q.x, w0);
+        hits += op.edge_peeked(v1, x, payload, q.y, w1);
+        hits += op.edge_peeked(v2, x, payload, q.z, w2);
+        hits += op.edge_peeked(v3, x, payload, q.w, w3);
+    } else {
+        hits += op.edge(v0, x, payload, q.x);
+        hits += op.edge(v1, x, payload, q.y);
+        hits += op.edge(v2, x, payload, q.z);
+        hits += op.edge(v3, x, payload, q.w);
+    }
+    return hits;
+}
+
 // Sweep of one row by `lanes` threads (a warp or a block; `t` = the
 // thread's rank among them).  Rows start on a 16-byte boundary in the
 // arenas (a block of 2^c >= 4 slots is aligned to its size), so each thread
 // reads four consecutive entries with one 16-byte load: a warp moves 128
 // entries, 512 bytes, per step, and a zero-copy row crosses the host link
-// in full 16-byte requests.  Entries past `deg` (still inside the block,
-// whose size is a multiple of 4) are masked.  A row that is not 16-byte
-// aligned (a caller's plain CSR) is read one entry per thread.  Every
-// thread of the group runs the same number of steps (Op::edge is
+// in full 16-byte requests.  The load of a thread's next step is issued
+// before the current step's entries are used, so on rows of several steps
+// the row reads overlap the state reads.  Entries past `deg` (still inside
+// the block, whose size is a multiple of 4) are masked.  A row that is not
+// 16-byte aligned (a caller's plain CSR) is read one entry per thread.
+// Every thread of the group runs the same number of steps (Op::edge is
 // warp-synchronous).
 template <uint32_t lanes, class Op, class P>
 __device__ __forceinline__ void sweep_row(const AdjView &view, const uint32_t *rp, uint32_t deg, uint32_t t,
                                           uint32_t x, P payload, const Op &op, ExpandCounters &cnt) {
     if ((reinterpret_cast<uintptr_t>(rp) & 15u) == 0) {
+        const uint4 tomb4 = make_uint4(kTomb, kTomb, kTomb, kTomb);
+        uint32_t k = 4u * t;
+        uint4 q = k < deg ? __ldg(reinterpret_cast<const uint4 *>(rp + k)) : tomb4;
         for (uint32_t base = 0; base < deg; base += 4u * lanes) {
-            const uint32_t k = base + 4u * t;
-            uint4 q = make_uint4(kTomb, kTomb, kTomb, kTomb);
-            if (k < deg) q = __ldg(reinterpret_cast<const uint4 *>(rp + k));
+            const uint32_t kn = k + 4u * lanes;
+            const uint4 qn = kn < deg ? __ldg(reinterpret_cast<const uint4 *>(rp + kn)) : tomb4;
             q.x = view.vid(q.x);
             q.y = view.vid(q.y);
             q.z = view.vid(q.z);
             q.w = view.vid(q.w);
-            cnt.hits += op.edge(k < deg && q.x != kTomb, x, payload, q.x);
-            cnt.hits += op.edge(k + 1u < deg && q.y != kTomb, x, payload, q.y);
-            cnt.hits += op.edge(k + 2u < deg && q.z != kTomb, x, payload, q.z);
-            cnt.hits += op.edge(k + 3u < deg && q.w != kTomb, x, payload, q.w);
+            cnt.hits += edge4(op, q, k, deg, x, payload);
+            q = qn;
+            k = kn;
         }
     } else {
         for (uint32_t base = 0; base < deg; base += lanes) {
@@ -107,6 +150,18 @@ __device__ __forceinline__ void sweep_row(const AdjView &view, const uint32_t *r
             cnt.hits += op.edge(valid && y != kTomb, x, payload, y);
         }
     }
+}
+
+// Rank of the calling thread in a block's share of a work list, dealt out
+// warp by warp: rank k sits in warp k mod (TPB/32), lane k / (TPB/32).  A
+// round often hands a block only a few items (a few dozen at most); with the
+// plain rank (= threadIdx.x) they would all land in warp 0, which would then
+// serve their rows one after another while the other warps idle.  Dealt
+// out, the first TPB/32 items go to different warps and their chains of
+// dependent row and state reads run side by side.
+template <int TPB>
+__device__ __forceinline__ uint32_t spread_rank() {
+    return (threadIdx.x & 31u) * static_cast<uint32_t>(TPB / 32) + (threadIdx.x >> 5);
 }
 
 // Op must provide: __device__ bool edge(bool valid, uint32_t x, P payload, uint32_t y) const;
@@ -190,26 +245,50 @@ __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint3
     sm.f_payload[wb + lane] = payload;
     sm.f_ptr[wb + lane] = mydeg ? view.at(off) : nullptr;
     __syncwarp();
-    for (uint32_t base = 0; base < total; base += 32u) {
-        const uint32_t e = base + lane;
-        const bool valid = e < total;
-        uint32_t ox = 0, y = 0;
-        P op_ = 0;
-        if (valid) {
-            // Last lane whose exclusive prefix is <= e owns edge e.
-            uint32_t lo = 0, hi = 32;
-            while (hi - lo > 1) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (sm.f_scan[wb + mid] <= e)
-                    lo = mid;
-                else
-                    hi = mid;
+    // Two entries per lane per step: both row reads, then (for ops with
+    // peek) both state reads, are in flight together.
+    for (uint32_t base = 0; base < total; base += 64u) {
+        uint32_t ox[2], y[2];
+        P pl[2];
+        bool valid[2];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const uint32_t e = base + 32u * j + lane;
+            valid[j] = e < total;
+            ox[j] = 0;
+            y[j] = 0;
+            pl[j] = 0;
+            if (valid[j]) {
+                // Last lane whose exclusive prefix is <= e owns edge e.
+                uint32_t lo = 0, hi = 32;
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (sm.f_scan[wb + mid] <= e)
+                        lo = mid;
+                    else
+                        hi = mid;
+                }
+                ox[j] = sm.f_x[wb + lo];
+                pl[j] = sm.f_payload[wb + lo];
+                y[j] = __ldg(sm.f_ptr[wb + lo] + (e - sm.f_scan[wb + lo]));
             }
-            ox = sm.f_x[wb + lo];
-            op_ = sm.f_payload[wb + lo];
-            y = view.vid(__ldg(sm.f_ptr[wb + lo] + (e - sm.f_scan[wb + lo])));
         }
-        cnt.hits += op.edge(valid && y != kTomb, ox, op_, y);
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            y[j] = valid[j] ? view.vid(y[j]) : 0u;
+            valid[j] = valid[j] && y[j] != kTomb;
+        }
+        if constexpr (has_peek<Op>::value) {
+            using W = decltype(op.peek(0u));
+            W w0{}, w1{};
+            if (valid[0]) w0 = op.peek(y[0]);
+            if (valid[1]) w1 = op.peek(y[1]);
+            cnt.hits += op.edge_peeked(valid[0], ox[0], pl[0], y[0], w0);
+            cnt.hits += op.edge_peeked(valid[1], ox[1], pl[1], y[1], w1);
+        } else {
+            cnt.hits += op.edge(valid[0], ox[0], pl[0], y[0]);
+            cnt.hits += op.edge(valid[1], ox[1], pl[1], y[1]);
+        }
     }
     __syncwarp();
 }

@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(kTpbPr) pr_converge(AdjView fwd, PrArrays<T> a
         if (!grid_barrier(st)) break;
         PrPushOp<T> op{a, a.queued, a.contrib, eps, (r & 1) ? a.q0 : a.q1, a.cnt + ((r + 1) % 3), a.cap, st};
         for (uint32_t base = 0; base < n_in; base += gridDim.x * kTpbPr) {
-            const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
+            const uint32_t i = base + spread_rank<kTpbPr>() * gridDim.x + blockIdx.x;
             bool has = i < n_in;
             uint32_t v = 0, deg = 0;
             uint64_t off = 0;
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(kTpbPr) pr_amend_scatter(AdjView fwd, PrArrays
     const uint32_t n = *count;
     PrPushOp<T> op{a, a.queued, contrib, eps, a.q0, a.cnt, a.cap, st};
     for (uint32_t base = 0; base < n; base += gridDim.x * kTpbPr) {
-        const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
+        const uint32_t i = base + spread_rank<kTpbPr>() * gridDim.x + blockIdx.x;
         bool has = i < n;
         uint32_t s = 0, deg = 0;
         uint64_t off = 0;
@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(kTpbPr) pr_amend_scatter64(AdjView fwd, const 
     const uint32_t n = *count;
     const PrAmendOp op{acc, contrib};
     for (uint32_t base = 0; base < n; base += gridDim.x * kTpbPr) {
-        const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
+        const uint32_t i = base + spread_rank<kTpbPr>() * gridDim.x + blockIdx.x;
         bool has = i < n;
         uint32_t s = 0, deg = 0;
         uint64_t off = 0;

@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(kTpbMs) ms_closure(AdjView fwd, uint32_t *dist
         }
         const Defer df{big.rows, big.cnt + (r % 3), big.cap, big.split};
         for (uint32_t base = 0; base < n_in; base += gridDim.x * kTpbMs) {
-            const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
+            const uint32_t i = base + spread_rank<kTpbMs>() * gridDim.x + blockIdx.x;
             bool has = i < n_in;
             uint32_t x = 0, deg = 0;
             uint64_t off = 0;

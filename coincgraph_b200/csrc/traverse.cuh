@@ -53,20 +53,27 @@ struct PushOp {
     uint32_t *q_count;
     uint32_t q_cap;
     Status *st;
+    const RowDesc *desc;  // rows of the queued vertices: prefetched into L2 for the next hop
 
-    __device__ __forceinline__ bool edge(bool valid, uint32_t x, uint32_t dx, uint32_t y) const {
+    __device__ __forceinline__ unsigned long long peek(uint32_t y) const { return __ldcg(state + y); }
+    __device__ __forceinline__ bool edge_peeked(bool valid, uint32_t x, uint32_t dx, uint32_t y,
+                                                unsigned long long sy) const {
         bool want = false, improved = false;
         if (valid) {
             const uint32_t nd = relax_value<A>(dx, x, y, ccs);
             const unsigned long long cand = pack(nd, x);
-            if (cand < __ldcg(state + y)) {
+            if (cand < sy) {
                 const unsigned long long old = atomicMin(state + y, cand);
                 improved = nd < val_of(old);
-                if (improved && __ldcg(qstamp + y) != tag) want = atomicExch(qstamp + y, tag) != tag;
+                if (improved) want = atomicExch(qstamp + y, tag) != tag;
             }
         }
+        if (want) prefetch_l2(desc + y);
         warp_enqueue(want, y, q_out, q_count, q_cap, st);
         return improved;
+    }
+    __device__ __forceinline__ bool edge(bool valid, uint32_t x, uint32_t dx, uint32_t y) const {
+        return edge_peeked(valid, x, dx, y, valid ? peek(y) : 0ull);
     }
 };
 
@@ -85,11 +92,16 @@ struct InvalOp {
     uint32_t *count;  // this round's append counter
     uint32_t cap;
     Status *st;
+    const RowDesc *desc;  // rows of the queued vertices: prefetched into L2 for the next hop
 
+    __device__ __forceinline__ unsigned long long peek(uint32_t z) const { return __ldcg(state + z); }
     __device__ __forceinline__ bool edge(bool valid, uint32_t x, uint32_t px, uint32_t z) const {
+        return edge_peeked(valid, x, px, z, valid ? peek(z) : 0ull);
+    }
+    __device__ __forceinline__ bool edge_peeked(bool valid, uint32_t x, uint32_t px, uint32_t z,
+                                                unsigned long long sz) const {
         bool want = false;
         if (valid) {
-            const unsigned long long sz = __ldcg(state + z);
             bool dep;
             if (A == kCc) {
                 const uint32_t vz = val_of(sz);
@@ -98,8 +110,9 @@ struct InvalOp {
             } else {
                 dep = par_of(sz) == x;
             }
-            if (dep && __ldcg(aff_stamp + z) != epoch) want = atomicExch(aff_stamp + z, epoch) != epoch;
+            if (dep) want = atomicExch(aff_stamp + z, epoch) != epoch;
         }
+        if (want) prefetch_l2(desc + z);
         warp_enqueue(want, z, list, count, cap, st);
         return want;
     }
@@ -116,20 +129,30 @@ struct PullOp {
     const uint32_t *aff_stamp;
     uint32_t epoch;
 
-    __device__ __forceinline__ bool edge(bool valid, uint32_t v, uint32_t, uint32_t u) const {
+    // Both words of u at once: bit 32 = u is invalidated, low half = u's value.
+    __device__ __forceinline__ unsigned long long peek(uint32_t u) const {
+        const uint32_t stamp = __ldcg(aff_stamp + u);
+        const uint32_t du = val_of(__ldcg(state + u));
+        return (stamp == epoch ? (1ull << 32) : 0ull) | du;
+    }
+    __device__ __forceinline__ bool edge_peeked(bool valid, uint32_t v, uint32_t, uint32_t u,
+                                                unsigned long long w) const {
         if (!valid) return false;
         unsigned long long cand;
-        if (__ldcg(aff_stamp + u) == epoch) {
+        if (w >> 32) {
             if (A != kCc) return false;
             cand = pack(cc_step(u << ccs, ccs), u);  // u restarts as its own seed
         } else {
-            const uint32_t du = val_of(__ldcg(state + u));
+            const uint32_t du = static_cast<uint32_t>(w);
             if (du == kInf) return false;
             cand = pack(relax_value<A>(du, u, v, ccs), u);
         }
         if (cand >= __ldcg(state + v)) return false;
         atomicMin(state + v, cand);
         return true;
+    }
+    __device__ __forceinline__ bool edge(bool valid, uint32_t v, uint32_t p, uint32_t u) const {
+        return edge_peeked(valid, v, p, u, valid ? peek(u) : 0ull);
     }
 };
 
@@ -149,11 +172,11 @@ struct BigList {
 };
 
 // Block-local sweeps.  After a block has relaxed its share of a round's
-// frontier, the vertices it improved (and that are not already queued for
-// the next round) go to a queue in its shared memory, and the block expands
-// them itself for up to `max_sweeps` more hops, synchronising with
-// __syncthreads only; what is left (or does not fit) goes to the next
-// round's frontier as usual.  On high-diameter graphs, whose rounds carry
+// frontier, the vertices it improved go to a queue in its shared memory, and
+// the block expands them itself for up to `max_sweeps` more hops,
+// synchronising with __syncthreads only (a vertex that is in the next
+// round's frontier by the time a sweep reads it is left to that round); what
+// is left (or does not fit) goes to the next round's frontier as usual.  On high-diameter graphs, whose rounds carry
 // small frontiers and cost a chain of dependent memory accesses plus a grid
 // barrier each, this covers several hops per grid round.  A vertex may then
 // be expanded by two blocks in one round (a redundant relaxation); the
@@ -173,18 +196,25 @@ struct LocalPushOp {
     uint32_t *lq;       // shared-memory queue of this sweep's output
     uint32_t *lq_n;
     Status *st;
+    const RowDesc *desc;  // rows of the queued vertices: prefetched into L2 for the next hop
 
+    __device__ __forceinline__ unsigned long long peek(uint32_t y) const { return __ldcg(state + y); }
     __device__ __forceinline__ bool edge(bool valid, uint32_t x, uint32_t dx, uint32_t y) const {
+        return edge_peeked(valid, x, dx, y, valid ? peek(y) : 0ull);
+    }
+    __device__ __forceinline__ bool edge_peeked(bool valid, uint32_t x, uint32_t dx, uint32_t y,
+                                                unsigned long long sy) const {
         bool want = false, improved = false;
         if (valid) {
             const uint32_t nd = relax_value<A>(dx, x, y, ccs);
             const unsigned long long cand = pack(nd, x);
-            if (cand < __ldcg(state + y)) {
+            if (cand < sy) {
                 const unsigned long long old = atomicMin(state + y, cand);
                 improved = nd < val_of(old);
-                want = improved && __ldcg(qstamp + y) != tag;
+                want = improved;  // a y already in the next frontier is skipped when the sweep reads it
             }
         }
+        if (want) prefetch_l2(desc + y);
         const uint32_t mask = __ballot_sync(kFull, want);
         bool spill = false;
         if (mask) {
@@ -233,16 +263,17 @@ __global__ void __launch_bounds__(kTpb, 4) push_closure(AdjView fwd, unsigned lo
         const uint32_t *in = (r & 1) ? fr.q1 : fr.q0;
         uint32_t *out = (r & 1) ? fr.q0 : fr.q1;
         uint32_t *out_cnt = fr.cnt + ((r + 1) % 3);
-        PushOp<A> op{ccs, state, qstamp, tag0 + r, out, out_cnt, fr.cap, st};
+        PushOp<A> op{ccs, state, qstamp, tag0 + r, out, out_cnt, fr.cap, st, fwd.desc};
         const Defer df{big.rows, big.cnt + (r % 3), big.cap, big.split};
         if (sweeps) {
             if (threadIdx.x == 0) lq_n[0] = 0;
             __syncthreads();
         }
         // Item i goes to block i mod gridDim.x, so small frontiers still
-        // spread over the whole grid.
+        // spread over the whole grid, and within the block to the warps in
+        // turn (spread_rank).
         for (uint32_t base = 0; base < n_in; base += gridDim.x * kTpb) {
-            const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
+            const uint32_t i = base + spread_rank<kTpb>() * gridDim.x + blockIdx.x;
             bool has = i < n_in;
             uint32_t x = 0, dx = 0, deg = 0;
             uint64_t off = 0;
@@ -258,7 +289,7 @@ __global__ void __launch_bounds__(kTpb, 4) push_closure(AdjView fwd, unsigned lo
             if (sweeps)
                 expand_rows<kTpb>(fwd, has, x, dx, off, deg,
                                   LocalPushOp<A>{ccs, state, qstamp, tag0 + r, out, out_cnt, fr.cap, lq[0], &lq_n[0],
-                                                 st},
+                                                 st, fwd.desc},
                                   sm, cnt, df);
             else
                 expand_rows<kTpb>(fwd, has, x, dx, off, deg, op, sm, cnt, df);
@@ -272,19 +303,20 @@ __global__ void __launch_bounds__(kTpb, 4) push_closure(AdjView fwd, unsigned lo
                 if (threadIdx.x == 0) lq_n[cur ^ 1u] = 0;
                 __syncthreads();
                 const LocalPushOp<A> lop{ccs, state, qstamp, tag0 + r, out, out_cnt, fr.cap, lq[cur ^ 1u],
-                                         &lq_n[cur ^ 1u], st};
+                                         &lq_n[cur ^ 1u], st, fwd.desc};
                 for (uint32_t base = 0; base < nl; base += kTpb) {
-                    const uint32_t i = base + threadIdx.x;
+                    const uint32_t i = base + spread_rank<kTpb>();
                     bool has = i < nl;
                     uint32_t x = 0, dx = 0, deg = 0;
                     uint64_t off = 0;
                     if (has) {
                         x = lq[cur][i];
                         dx = val_of(__ldcg(state + x));
+                        const bool queued = __ldcg(qstamp + x) == tag0 + r;  // the next round expands it
                         const RowDesc d = fwd.desc[x];
                         deg = d.len;
                         off = d.off;
-                        has = dx != kInf && deg > 0;
+                        has = dx != kInf && deg > 0 && !queued;
                         if (has && seg_hot) atomicAdd(seg_hot + (off >> kSegShift), deg);
                     }
                     expand_rows<kTpb>(fwd, has, x, dx, off, deg, lop, sm, cnt, df);
@@ -337,11 +369,16 @@ struct LocalInvalOp {
     uint32_t *lq;
     uint32_t *lq_n;
     Status *st;
+    const RowDesc *desc;  // rows of the queued vertices: prefetched into L2 for the next hop
 
+    __device__ __forceinline__ unsigned long long peek(uint32_t z) const { return __ldcg(state + z); }
     __device__ __forceinline__ bool edge(bool valid, uint32_t x, uint32_t px, uint32_t z) const {
+        return edge_peeked(valid, x, px, z, valid ? peek(z) : 0ull);
+    }
+    __device__ __forceinline__ bool edge_peeked(bool valid, uint32_t x, uint32_t px, uint32_t z,
+                                                unsigned long long sz) const {
         bool want = false;
         if (valid) {
-            const unsigned long long sz = __ldcg(state + z);
             bool dep;
             if (A == kCc) {
                 const uint32_t vz = val_of(sz);
@@ -350,8 +387,9 @@ struct LocalInvalOp {
             } else {
                 dep = par_of(sz) == x;
             }
-            if (dep && __ldcg(aff_stamp + z) != epoch) want = atomicExch(aff_stamp + z, epoch) != epoch;
+            if (dep) want = atomicExch(aff_stamp + z, epoch) != epoch;
         }
+        if (want) prefetch_l2(desc + z);
         const uint32_t mask = __ballot_sync(kFull, want);
         bool spill = false;
         if (mask) {
@@ -397,7 +435,8 @@ __global__ void __launch_bounds__(kTpb, 4) inval_closure(AdjView fwd, unsigned l
             cnt3[(r + 2) % 3] = 0;
             big.cnt[(r + 2) % 3] = 0;
         }
-        InvalOp<A> op{ccs, state, aff_stamp, epoch, list + hi, cnt3 + ((r + 1) % 3), cap > hi ? cap - hi : 0u, st};
+        InvalOp<A> op{ccs, state, aff_stamp, epoch, list + hi, cnt3 + ((r + 1) % 3), cap > hi ? cap - hi : 0u, st,
+                      fwd.desc};
         const Defer df{big.rows, big.cnt + (r % 3), big.cap, big.split};
         const uint32_t n_in = hi - lo;
         // Sweeps only for small frontiers (a few items per block): on R-MAT
@@ -409,7 +448,7 @@ __global__ void __launch_bounds__(kTpb, 4) inval_closure(AdjView fwd, unsigned l
             __syncthreads();
         }
         for (uint32_t base = 0; base < n_in; base += gridDim.x * kTpb) {
-            const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
+            const uint32_t i = base + spread_rank<kTpb>() * gridDim.x + blockIdx.x;
             bool has = i < n_in;
             uint32_t x = 0, px = 0, deg = 0;
             uint64_t off = 0;
@@ -425,7 +464,7 @@ __global__ void __launch_bounds__(kTpb, 4) inval_closure(AdjView fwd, unsigned l
             if (sweeps)
                 expand_rows<kTpb>(fwd, has, x, px, off, deg,
                                   LocalInvalOp<A>{ccs, state, aff_stamp, epoch, op.list, op.count, op.cap, lq[0],
-                                                  &lq_n[0], st},
+                                                  &lq_n[0], st, fwd.desc},
                                   sm, c, df);
             else
                 expand_rows<kTpb>(fwd, has, x, px, off, deg, op, sm, c, df);
@@ -439,9 +478,9 @@ __global__ void __launch_bounds__(kTpb, 4) inval_closure(AdjView fwd, unsigned l
                 if (threadIdx.x == 0) lq_n[cur ^ 1u] = 0;
                 __syncthreads();
                 const LocalInvalOp<A> lop{ccs, state, aff_stamp, epoch, op.list, op.count, op.cap, lq[cur ^ 1u],
-                                          &lq_n[cur ^ 1u], st};
+                                          &lq_n[cur ^ 1u], st, fwd.desc};
                 for (uint32_t base = 0; base < nl; base += kTpb) {
-                    const uint32_t i = base + threadIdx.x;
+                    const uint32_t i = base + spread_rank<kTpb>();
                     bool has = i < nl;
                     uint32_t x = 0, px = 0, deg = 0;
                     uint64_t off = 0;
@@ -546,7 +585,7 @@ __global__ void reset_affected(const uint32_t *list, const uint32_t *total, unsi
 }
 
 template <int A>
-__global__ void __launch_bounds__(kTpb) pull_repair(AdjView rev, unsigned long long *state, const uint32_t *aff_stamp,
+__global__ void __launch_bounds__(kTpb, 4) pull_repair(AdjView rev, unsigned long long *state, const uint32_t *aff_stamp,
                                                     const uint32_t *epoch_p, const uint32_t *list,
                                                     const uint32_t *total, BigList big, Status *st) {
     __shared__ ExpandSmem<kTpb> sm;
@@ -555,7 +594,7 @@ __global__ void __launch_bounds__(kTpb) pull_repair(AdjView rev, unsigned long l
     PullOp<A> op{(A == kCc) ? st->cc_shift : 0u, state, aff_stamp, *epoch_p};
     const Defer df{big.rows, big.cnt, big.cap, big.split};
     for (uint32_t base = 0; base < n; base += gridDim.x * kTpb) {
-        const uint32_t i = base + threadIdx.x * gridDim.x + blockIdx.x;
+        const uint32_t i = base + spread_rank<kTpb>() * gridDim.x + blockIdx.x;
         bool has = i < n;
         uint32_t v = 0, deg = 0;
         uint64_t off = 0;
