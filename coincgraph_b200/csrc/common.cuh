@@ -201,6 +201,38 @@ __device__ __forceinline__ void warp_enqueue(bool want, uint32_t item, uint32_t 
     }
 }
 
+// Append up to N items per lane (item[j] where want[j]) with one warp scan
+// and one atomic per warp.
+template <int N>
+__device__ __forceinline__ void warp_enqueue_n(const bool (&want)[N], const uint32_t (&item)[N], uint32_t *queue,
+                                               uint32_t *count, uint32_t capacity, Status *st) {
+    uint32_t c = 0;
+#pragma unroll
+    for (int j = 0; j < N; ++j) c += want[j] ? 1u : 0u;
+    if (!__any_sync(kFull, c != 0u)) return;
+    const uint32_t lane = lane_id();
+    uint32_t incl = c;
+#pragma unroll
+    for (uint32_t o = 1; o < 32u; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+    }
+    uint32_t base = 0;
+    if (lane == 31) base = atomicAdd(count, incl);
+    base = __shfl_sync(kFull, base, 31);
+    uint32_t pos = base + incl - c;
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        if (want[j]) {
+            if (pos < capacity)
+                queue[pos] = item[j];
+            else
+                set_error(st, kErrQueue, pos);
+            ++pos;
+        }
+    }
+}
+
 // Warp-aggregated counter add.
 __device__ __forceinline__ void warp_count(unsigned long long *counter, uint32_t value) {
     uint32_t sum = __reduce_add_sync(kFull, value);

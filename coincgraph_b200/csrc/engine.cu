@@ -88,11 +88,17 @@ inline uint32_t host_class(uint64_t deg) {
 
 // Initial arena layout: one region per class (largest classes first, each
 // region segment aligned), rows in vertex order inside a region.
+// Rows of at most 2^kSmallRowClass entries are "small" (one warp expands
+// them; larger rows take the whole block): most vertices, and most rows a
+// traversal reads, each read a short dependent access.
+constexpr uint32_t kSmallRowClass = 8;
+
 struct Layout {
     std::vector<RowDesc> desc;
     unsigned long long cur_next[kNumClasses] = {};
     unsigned long long cur_end[kNumClasses] = {};
     uint64_t used_segs = 0;
+    uint64_t small_segs = 0;  // the last segments, which hold the small rows
 };
 
 Layout plan_layout(uint32_t n, const uint32_t *deg) {
@@ -115,6 +121,7 @@ Layout plan_layout(uint32_t n, const uint32_t *deg) {
             segs = count[c] << (c - kSegShift);
         }
         seg += segs;
+        if (static_cast<uint32_t>(c) <= kSmallRowClass) L.small_segs += segs;
     }
     L.used_segs = seg;
     uint64_t cursor[kNumClasses];
@@ -842,6 +849,7 @@ struct cig_handle {
         if (const char *e = std::getenv("CIG_SPLIT_DEG")) tune.split = std::max(32, std::atoi(e));
         if (const char *e = std::getenv("CIG_INC_BLOCKS_PER_SM")) tune.inc_per_sm = std::max(0, std::atoi(e));
         if (const char *e = std::getenv("CIG_LOCAL_SWEEPS")) local_sweeps = static_cast<uint32_t>(std::max(0, std::atoi(e)));
+        if (const char *e = std::getenv("CIG_CACHE_SMALL_PCT")) cache_small_pct = std::min(100.0, std::max(0.0, std::atof(e)));
         if (opt.flags & CIG_FLAG_NO_GRAPHS) use_graphs = false;
         if (const char *e = std::getenv("CIG_GRAPHS")) use_graphs = std::atoi(e) != 0;
         if (const char *e = std::getenv("CIG_MERGE_PUSH")) merge_push = std::atoi(e) != 0;
@@ -1136,8 +1144,7 @@ struct cig_handle {
         CK(cudaMemcpy(fwd.desc, L.desc.data(), n * sizeof(RowDesc), cudaMemcpyHostToDevice));
         upload_alloc(fwd, L);
 
-        // HBM edge cache: whole segments, initially the first ones in arena order
-        // (largest row classes first).
+        // HBM edge cache: whole segments (initial choice below).
         uint64_t budget_slots;
         if (opt.cache_compat) {
             const long long c = static_cast<long long>(opt.cache_gib);
@@ -1155,14 +1162,31 @@ struct cig_handle {
         refresh = cache_slots > 0 && !(opt.flags & CIG_FLAG_NO_CACHE_REFRESH);
         const uint64_t filled = std::min<uint64_t>(cache_slots, fwd.seg_used);
         resident = refresh ? filled : cache_slots;
+        // Initially resident: the small rows first (the last segments), then
+        // the largest classes (the first segments) while slots last; the
+        // middle classes start in host memory.  A small row costs a
+        // traversal one dependent host access per read and most reads are of
+        // small rows, while a large row crosses the link in long requests but
+        // carries the most bytes; the rows between gain the least from HBM.
+        // CIG_CACHE_SMALL_PCT=p instead gives the last segments p % of the
+        // slots (0: the first segments only).
+        uint64_t small = std::min<uint64_t>(filled, L.small_segs);
+        if (cache_small_pct >= 0.0)
+            small = std::min<uint64_t>(filled, static_cast<uint64_t>(filled * cache_small_pct / 100.0));
+        if (!refresh) small = 0;
+        const uint64_t big = filled - small;
+        auto seg_of_slot = [&](uint64_t i) { return i < big ? i : fwd.seg_used - small + (i - big); };
         if (cache_slots) {
             dmalloc(fwd.dev, cache_slots * kSegEdges);
-            if (filled)
-                CK(cudaMemcpy(fwd.dev, fwd.host, filled * kSegEdges * sizeof(uint32_t), cudaMemcpyHostToDevice));
+            const size_t seg_bytes = kSegEdges * sizeof(uint32_t);
+            if (big) CK(cudaMemcpy(fwd.dev, fwd.host, big * seg_bytes, cudaMemcpyHostToDevice));
+            if (small)
+                CK(cudaMemcpy(fwd.dev + big * kSegEdges, fwd.host + (fwd.seg_used - small) * kSegEdges,
+                              small * seg_bytes, cudaMemcpyHostToDevice));
         }
         {
             std::vector<int32_t> slot(fwd.seg_total, -1);
-            for (uint64_t s = 0; s < resident; ++s) slot[s] = static_cast<int32_t>(s);
+            for (uint64_t i = 0; i < resident; ++i) slot[seg_of_slot(i)] = static_cast<int32_t>(i);
             dmalloc(fwd.seg_slot, fwd.seg_total);
             CK(cudaMemcpy(fwd.seg_slot, slot.data(), slot.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
             dmalloc(fwd.seg_dirty, fwd.seg_total);
@@ -1174,7 +1198,7 @@ struct cig_handle {
             if (const char *e = std::getenv("CIG_CACHE_ADMIT_SCORE")) admit_score = static_cast<uint32_t>(std::atol(e));
             if (const char *e = std::getenv("CIG_CACHE_COLD_SCORE")) cold_score = static_cast<uint32_t>(std::atol(e));
             std::vector<int32_t> owner(cache_slots, -1);
-            for (uint64_t s = 0; s < filled; ++s) owner[s] = static_cast<int32_t>(s);
+            for (uint64_t i = 0; i < filled; ++i) owner[i] = static_cast<int32_t>(seg_of_slot(i));
             std::vector<uint32_t> stack;
             for (uint64_t k = cache_slots; k-- > filled;) stack.push_back(static_cast<uint32_t>(k));
             dmalloc(slot_seg, cache_slots);
@@ -1336,6 +1360,10 @@ struct cig_handle {
         prof_end(p);
     }
     uint32_t local_sweeps = 8;  // block-local hops per closure round (CIG_LOCAL_SWEEPS; 0 = off)
+    // Share of the initially resident slots given to the last segments of the
+    // arena (the smallest row classes), in percent (CIG_CACHE_SMALL_PCT); a
+    // negative value: the segments of the small row classes.
+    double cache_small_pct = -1.0;
     // Whole batches run one push closure (after the insertions) instead of
     // one per phase (CIG_MERGE_PUSH=0: one per phase, as the per-phase calls).
     bool merge_push = true;

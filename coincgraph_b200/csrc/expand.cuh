@@ -85,31 +85,49 @@ struct has_peek : std::false_type {};
 template <class Op>
 struct has_peek<Op, std::void_t<decltype(std::declval<const Op &>().peek(0u))>> : std::true_type {};
 
+// Ops that declare kMulti also take a thread's N entries at once
+// (edges<N>(valid, x, payload, y, peeked)): their atomics are then in flight
+// together and their queue appends share one warp scan, instead of N
+// rounds of atomic, ballot and append.
+template <class Op, class = void>
+struct has_multi : std::false_type {};
+template <class Op>
+struct has_multi<Op, std::void_t<decltype(Op::kMulti)>> : std::true_type {};
+
+// N entries of one thread: entry j is edge x[j] -> y[j] with payload pl[j],
+// live when v[j].
+template <int N, class Op, class P>
+__device__ __forceinline__ uint32_t edges_n(const Op &op, const bool (&v)[N], const uint32_t (&x)[N],
+                                            const P (&pl)[N], const uint32_t (&y)[N]) {
+    uint32_t hits = 0;
+    if constexpr (has_peek<Op>::value) {
+        using W = decltype(op.peek(0u));
+        W w[N];
+#pragma unroll
+        for (int j = 0; j < N; ++j) w[j] = v[j] ? op.peek(y[j]) : W{};
+        if constexpr (has_multi<Op>::value) {
+            hits = op.template edges<N>(v, x, pl, y, w);
+        } else {
+#pragma unroll
+            for (int j = 0; j < N; ++j) hits += op.edge_peeked(v[j], x[j], pl[j], y[j], w[j]);
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < N; ++j) hits += op.edge(v[j], x[j], pl[j], y[j]);
+    }
+    return hits;
+}
+
 // The four entries of a 16-byte row load: entry j is live when it lies
 // before `deg` (relative index k + j) and is not a tombstone.
 template <class Op, class P>
 __device__ __forceinline__ uint32_t edge4(const Op &op, uint4 q, uint32_t k, uint32_t deg, uint32_t x, P payload) {
-    const bool v0 = k < deg && q.x != kTomb, v1 = k + 1u < deg && q.y != kTomb;
-    const bool v2 = k + 2u < deg && q.z != kTomb, v3 = k + 3u < deg && q.w != kTomb;
-    uint32_t hits = 0;
-    if constexpr (has_peek<Op>::value) {
-        using W = decltype(op.peek(0u));
-        W w0{}, w1{}, w2{}, w3{};
-        if (v0) w0 = op.peek(q.x);
-        if (v1) w1 = op.peek(q.y);
-        if (v2) w2 = op.peek(q.z);
-        if (v3) w3 = op.peek(q.w);
-        hits += op.edge_peeked(v0, x, payload, q.x, w0);
-        hits += op.edge_peeked(v1, x, payload, q.y, w1);
-        hits += op.edge_peeked(v2, x, payload, q.z, w2);
-        hits += op.edge_peeked(v3, x, payload, q.w, w3);
-    } else {
-        hits += op.edge(v0, x, payload, q.x);
-        hits += op.edge(v1, x, payload, q.y);
-        hits += op.edge(v2, x, payload, q.z);
-        hits += op.edge(v3, x, payload, q.w);
-    }
-    return hits;
+    const bool v[4] = {k < deg && q.x != kTomb, k + 1u < deg && q.y != kTomb, k + 2u < deg && q.z != kTomb,
+                       k + 3u < deg && q.w != kTomb};
+    const uint32_t xs[4] = {x, x, x, x};
+    const P ps[4] = {payload, payload, payload, payload};
+    const uint32_t ys[4] = {q.x, q.y, q.z, q.w};
+    return edges_n<4>(op, v, xs, ps, ys);
 }
 
 // Sweep of one row by `lanes` threads (a warp or a block; `t` = the
@@ -127,7 +145,57 @@ __device__ __forceinline__ uint32_t edge4(const Op &op, uint4 q, uint32_t k, uin
 template <uint32_t lanes, class Op, class P>
 __device__ __forceinline__ void sweep_row(const AdjView &view, const uint32_t *rp, uint32_t deg, uint32_t t,
                                           uint32_t x, P payload, const Op &op, ExpandCounters &cnt) {
-    if ((reinterpret_cast<uintptr_t>(rp) & 15u) == 0) {
+    const bool aligned = (reinterpret_cast<uintptr_t>(rp) & 15u) == 0;
+    if constexpr (has_peek<Op>::value && has_multi<Op>::value) {
+        if (aligned) {
+            // Two steps in flight: while a step's entries are relaxed, the
+            // next step's state words are being read and the one after
+            // that's row entries.
+            using W = decltype(op.peek(0u));
+            const uint4 tomb4 = make_uint4(kTomb, kTomb, kTomb, kTomb);
+            const uint32_t xs[4] = {x, x, x, x};
+            const P ps[4] = {payload, payload, payload, payload};
+            auto live = [&](uint4 &q, uint32_t k, bool (&v)[4], uint32_t (&ys)[4]) {
+                ys[0] = view.vid(q.x);
+                ys[1] = view.vid(q.y);
+                ys[2] = view.vid(q.z);
+                ys[3] = view.vid(q.w);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) v[j] = k + j < deg && ys[j] != kTomb;
+            };
+            uint32_t k = 4u * t;
+            uint4 q = k < deg ? __ldg(reinterpret_cast<const uint4 *>(rp + k)) : tomb4;
+            bool v[4];
+            uint32_t ys[4];
+            W w[4];
+            live(q, k, v, ys);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) w[j] = v[j] ? op.peek(ys[j]) : W{};
+            uint32_t kn = k + 4u * lanes;
+            uint4 qn = kn < deg ? __ldg(reinterpret_cast<const uint4 *>(rp + kn)) : tomb4;
+            for (uint32_t base = 0; base < deg; base += 4u * lanes) {
+                bool vn[4];
+                uint32_t yn[4];
+                W wn[4];
+                live(qn, kn, vn, yn);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) wn[j] = vn[j] ? op.peek(yn[j]) : W{};
+                const uint32_t knn = kn + 4u * lanes;
+                const uint4 qnn = knn < deg ? __ldg(reinterpret_cast<const uint4 *>(rp + knn)) : tomb4;
+                cnt.hits += op.template edges<4>(v, xs, ps, ys, w);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    v[j] = vn[j];
+                    ys[j] = yn[j];
+                    w[j] = wn[j];
+                }
+                qn = qnn;
+                kn = knn;
+            }
+            return;
+        }
+    }
+    if (aligned) {
         const uint4 tomb4 = make_uint4(kTomb, kTomb, kTomb, kTomb);
         uint32_t k = 4u * t;
         uint4 q = k < deg ? __ldg(reinterpret_cast<const uint4 *>(rp + k)) : tomb4;
@@ -278,17 +346,7 @@ __device__ __forceinline__ void expand_rows(const AdjView &view, bool has, uint3
             y[j] = valid[j] ? view.vid(y[j]) : 0u;
             valid[j] = valid[j] && y[j] != kTomb;
         }
-        if constexpr (has_peek<Op>::value) {
-            using W = decltype(op.peek(0u));
-            W w0{}, w1{};
-            if (valid[0]) w0 = op.peek(y[0]);
-            if (valid[1]) w1 = op.peek(y[1]);
-            cnt.hits += op.edge_peeked(valid[0], ox[0], pl[0], y[0], w0);
-            cnt.hits += op.edge_peeked(valid[1], ox[1], pl[1], y[1], w1);
-        } else {
-            cnt.hits += op.edge(valid[0], ox[0], pl[0], y[0]);
-            cnt.hits += op.edge(valid[1], ox[1], pl[1], y[1]);
-        }
+        cnt.hits += edges_n<2>(op, valid, ox, pl, y);
     }
     __syncwarp();
 }

@@ -75,13 +75,48 @@ struct PushOp {
     __device__ __forceinline__ bool edge(bool valid, uint32_t x, uint32_t dx, uint32_t y) const {
         return edge_peeked(valid, x, dx, y, valid ? peek(y) : 0ull);
     }
+    static constexpr bool kMulti = true;
+    template <int N>
+    __device__ __forceinline__ uint32_t edges(const bool (&v)[N], const uint32_t (&x)[N], const uint32_t (&dx)[N],
+                                              const uint32_t (&y)[N], const unsigned long long (&sy)[N]) const {
+        unsigned long long cand[N], old[N];
+        bool want[N];
+        uint32_t hits = 0;
+#pragma unroll
+        for (int j = 0; j < N; ++j) cand[j] = pack(relax_value<A>(dx[j], x[j], y[j], ccs), x[j]);
+#pragma unroll
+        for (int j = 0; j < N; ++j) old[j] = (v[j] && cand[j] < sy[j]) ? atomicMin(state + y[j], cand[j]) : 0ull;
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            const bool improved = v[j] && cand[j] < sy[j] && val_of(cand[j]) < val_of(old[j]);
+            hits += improved ? 1u : 0u;
+            want[j] = improved && atomicExch(qstamp + y[j], tag) != tag;
+        }
+#pragma unroll
+        for (int j = 0; j < N; ++j)
+            if (want[j]) prefetch_l2(desc + y[j]);
+        warp_enqueue_n<N>(want, y, q_out, q_count, q_cap, st);
+        return hits;
+    }
 };
 
-// Deletion dependency of an out-neighbour z of an invalidated vertex x.
-// BFS/SSSP: z's parent is x (IsDeletionDependency, api.cuh:43-49; the packed
-// state makes every parent tight).  CC: equal labels and z is not its own
-// seed (hybrid_cc.cu:45-49), since equal-label cycles may hold parents that
-// do not lead back to the seed.
+// Deletion dependency of an out-neighbour z (state word sz) of an
+// invalidated vertex x (value px).  BFS/SSSP: z's parent is x
+// (IsDeletionDependency, api.cuh:43-49; the packed state makes every parent
+// tight).  CC: equal labels and z is not its own seed (hybrid_cc.cu:45-49),
+// since equal-label cycles may hold parents that do not lead back to the
+// seed.
+template <int A>
+__device__ __forceinline__ bool inval_dep(uint32_t ccs, uint32_t x, uint32_t px, uint32_t z, unsigned long long sz) {
+    if (A == kCc) {
+        const uint32_t vz = val_of(sz);
+        return z != x &&
+               (par_of(sz) == x || (cc_saturated(vz, ccs) && (vz >> ccs) == (px >> ccs) && (vz >> ccs) < z));
+    }
+    return par_of(sz) == x;
+}
+
+// Claims the out-neighbours of invalidated vertices that depend on them.
 template <int A>
 struct InvalOp {
     uint32_t ccs;
@@ -101,20 +136,29 @@ struct InvalOp {
     __device__ __forceinline__ bool edge_peeked(bool valid, uint32_t x, uint32_t px, uint32_t z,
                                                 unsigned long long sz) const {
         bool want = false;
-        if (valid) {
-            bool dep;
-            if (A == kCc) {
-                const uint32_t vz = val_of(sz);
-                dep = z != x && (par_of(sz) == x || (cc_saturated(vz, ccs) && (vz >> ccs) == (px >> ccs) &&
-                                                     (vz >> ccs) < z));
-            } else {
-                dep = par_of(sz) == x;
-            }
-            if (dep) want = atomicExch(aff_stamp + z, epoch) != epoch;
-        }
+        if (valid && inval_dep<A>(ccs, x, px, z, sz)) want = atomicExch(aff_stamp + z, epoch) != epoch;
         if (want) prefetch_l2(desc + z);
         warp_enqueue(want, z, list, count, cap, st);
         return want;
+    }
+    static constexpr bool kMulti = true;
+    template <int N>
+    __device__ __forceinline__ uint32_t edges(const bool (&v)[N], const uint32_t (&x)[N], const uint32_t (&px)[N],
+                                              const uint32_t (&z)[N], const unsigned long long (&sz)[N]) const {
+        bool want[N];
+        uint32_t hits = 0;
+#pragma unroll
+        for (int j = 0; j < N; ++j) want[j] = v[j] && inval_dep<A>(ccs, x[j], px[j], z[j], sz[j]);
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            want[j] = want[j] && atomicExch(aff_stamp + z[j], epoch) != epoch;
+            hits += want[j] ? 1u : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < N; ++j)
+            if (want[j]) prefetch_l2(desc + z[j]);
+        warp_enqueue_n<N>(want, z, list, count, cap, st);
+        return hits;
     }
 };
 
@@ -233,6 +277,51 @@ struct LocalPushOp {
         }
         warp_enqueue(spill, y, q_out, q_count, q_cap, st);
         return improved;
+    }
+    static constexpr bool kMulti = true;
+    template <int N>
+    __device__ __forceinline__ uint32_t edges(const bool (&v)[N], const uint32_t (&x)[N], const uint32_t (&dx)[N],
+                                              const uint32_t (&y)[N], const unsigned long long (&sy)[N]) const {
+        unsigned long long cand[N], old[N];
+        bool want[N], spill[N];
+        uint32_t hits = 0, c = 0;
+#pragma unroll
+        for (int j = 0; j < N; ++j) cand[j] = pack(relax_value<A>(dx[j], x[j], y[j], ccs), x[j]);
+#pragma unroll
+        for (int j = 0; j < N; ++j) old[j] = (v[j] && cand[j] < sy[j]) ? atomicMin(state + y[j], cand[j]) : 0ull;
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            want[j] = v[j] && cand[j] < sy[j] && val_of(cand[j]) < val_of(old[j]);
+            hits += want[j] ? 1u : 0u;
+            c += want[j] ? 1u : 0u;
+            spill[j] = false;
+            if (want[j]) prefetch_l2(desc + y[j]);
+        }
+        if (__any_sync(kFull, c != 0u)) {
+            const uint32_t lane = lane_id();
+            uint32_t incl = c;
+#pragma unroll
+            for (uint32_t o = 1; o < 32u; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(kFull, incl, o);
+                if (lane >= o) incl += t;
+            }
+            uint32_t base = 0;
+            if (lane == 31) base = atomicAdd(lq_n, incl);
+            base = __shfl_sync(kFull, base, 31);
+            uint32_t pos = base + incl - c;
+#pragma unroll
+            for (int j = 0; j < N; ++j) {
+                if (want[j]) {
+                    if (pos < kLocalCap)
+                        lq[pos] = y[j];
+                    else
+                        spill[j] = atomicExch(qstamp + y[j], tag) != tag;
+                    ++pos;
+                }
+            }
+        }
+        warp_enqueue_n<N>(spill, y, q_out, q_count, q_cap, st);
+        return hits;
     }
 };
 
@@ -378,17 +467,7 @@ struct LocalInvalOp {
     __device__ __forceinline__ bool edge_peeked(bool valid, uint32_t x, uint32_t px, uint32_t z,
                                                 unsigned long long sz) const {
         bool want = false;
-        if (valid) {
-            bool dep;
-            if (A == kCc) {
-                const uint32_t vz = val_of(sz);
-                dep = z != x && (par_of(sz) == x || (cc_saturated(vz, ccs) && (vz >> ccs) == (px >> ccs) &&
-                                                     (vz >> ccs) < z));
-            } else {
-                dep = par_of(sz) == x;
-            }
-            if (dep) want = atomicExch(aff_stamp + z, epoch) != epoch;
-        }
+        if (valid && inval_dep<A>(ccs, x, px, z, sz)) want = atomicExch(aff_stamp + z, epoch) != epoch;
         if (want) prefetch_l2(desc + z);
         const uint32_t mask = __ballot_sync(kFull, want);
         bool spill = false;
@@ -408,6 +487,48 @@ struct LocalInvalOp {
         }
         warp_enqueue(spill, z, list, count, cap, st);
         return want;
+    }
+    static constexpr bool kMulti = true;
+    template <int N>
+    __device__ __forceinline__ uint32_t edges(const bool (&v)[N], const uint32_t (&x)[N], const uint32_t (&px)[N],
+                                              const uint32_t (&z)[N], const unsigned long long (&sz)[N]) const {
+        bool want[N], spill[N];
+        uint32_t hits = 0, c = 0;
+#pragma unroll
+        for (int j = 0; j < N; ++j) want[j] = v[j] && inval_dep<A>(ccs, x[j], px[j], z[j], sz[j]);
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            want[j] = want[j] && atomicExch(aff_stamp + z[j], epoch) != epoch;
+            hits += want[j] ? 1u : 0u;
+            c += want[j] ? 1u : 0u;
+            spill[j] = false;
+            if (want[j]) prefetch_l2(desc + z[j]);
+        }
+        if (__any_sync(kFull, c != 0u)) {
+            const uint32_t lane = lane_id();
+            uint32_t incl = c;
+#pragma unroll
+            for (uint32_t o = 1; o < 32u; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(kFull, incl, o);
+                if (lane >= o) incl += t;
+            }
+            uint32_t base = 0;
+            if (lane == 31) base = atomicAdd(lq_n, incl);
+            base = __shfl_sync(kFull, base, 31);
+            uint32_t pos = base + incl - c;
+#pragma unroll
+            for (int j = 0; j < N; ++j) {
+                if (want[j]) {
+                    if (pos < kLocalCap)
+                        lq[pos] = z[j];
+                    else
+                        spill[j] = true;
+                    ++pos;
+                }
+            }
+        }
+        warp_enqueue_n<N>(spill, z, list, count, cap, st);
+        return hits;
     }
 };
 

@@ -168,6 +168,18 @@ def test_segment_table_churn(algo, monkeypatch):
     assert sum(s["cache_segments_loaded"] for s in stats) > 0
 
 
+@pytest.mark.parametrize("small_pct", [None, 0, 50, 100])
+def test_split_initial_residency(small_pct, monkeypatch):
+    """The initially resident slots hold the last segments of the arena (the
+    small row classes; by default as many as there are, else the given
+    share of the slots) and the first ones: values and rows stay exact
+    against the oracle, also while the segment table evicts and admits."""
+    if small_pct is not None:
+        monkeypatch.setenv("CIG_CACHE_SMALL_PCT", str(small_pct))
+    monkeypatch.setenv("CIG_CACHE_ADMIT_SCORE", "64")
+    run_case_whole_batches(rmat_case(14, 5, 2000, 2000, seed_offset=16), "sssp", 8 * ONE_SEGMENT_GIB)
+
+
 @pytest.mark.parametrize("algo", ["bfs", "sssp", "cc"])
 def test_batched_form_equals_single_batches(algo):
     """cig_apply_batches_device (uneven batch sizes, one synchronisation)
