@@ -671,7 +671,65 @@ __device__ __forceinline__ uint32_t del_index_key(const AdjView &view, RowDesc *
     return 1u;
 }
 
-__global__ void del_index(AdjView view, RowDesc *desc, const unsigned long long *keys, Groups gr,
+// The keys of one lane, N at a time (live[j]: key j is served): the key,
+// descriptor, first index probe and its value slot of every key are read
+// before any of them is used, so the lane waits for one chain of dependent
+// loads instead of N.  The first probe almost always decides (the tables
+// stay at most half full); a collision continues with idx_find_from.
+template <int N>
+__device__ __forceinline__ uint32_t del_index_keys(const AdjView &view, RowDesc *desc,
+                                                   const unsigned long long *keys, const uint32_t (&ks)[N],
+                                                   const bool (&live)[N], uint32_t *firstpos, const PosIndex &ix,
+                                                   Status *st) {
+    unsigned long long key[N], slot[N], seen[N];
+    RowDesc d[N];
+    uint2 e[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) key[j] = live[j] ? keys[ks[j]] : 0ull;
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        const uint32_t u = key_src(key[j]);
+        if (live[j]) d[j] = desc[u];
+        key[j] = (static_cast<unsigned long long>(u) << 32) | key_low(key[j]);
+        slot[j] = idx_mix(key[j]) & ix.mask;
+        seen[j] = kIdxEmpty + 0ull;
+        if (live[j]) seen[j] = *reinterpret_cast<volatile unsigned long long *>(ix.keys + slot[j]);
+        e[j] = live[j] ? ix.val[slot[j]] : make_uint2(0u, 0u);
+    }
+    uint32_t removed = 0;
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        if (!live[j]) continue;
+        if (seen[j] != key[j]) {
+            if (seen[j] == kIdxEmpty) continue;  // not in the row: a missing delete
+            slot[j] = idx_find_from(ix, key[j], (slot[j] + 1) & ix.mask, 1);
+            if (slot[j] == ~0ull) continue;
+            e[j] = ix.val[slot[j]];
+        }
+        const uint32_t u = static_cast<uint32_t>(key[j] >> 32), v = static_cast<uint32_t>(key[j]);
+        if (e[j].y == 0u || e[j].x >= d[j].len) {
+            if (e[j].y != 0u) set_error(st, kErrInternal, 0x1d2u);
+            continue;
+        }
+        firstpos[ks[j]] = e[j].x | kApplied;
+        write_slot(view, d[j].off + e[j].x, kTomb);
+        atomicAdd(&desc[u].meta, 1u << 6);
+        if (e[j].y == 1u) {
+            ix.val[slot[j]] = make_uint2(kInf, 0u);
+            ix.keys[slot[j]] = kIdxDeleted;
+        } else {
+            uint32_t q = e[j].x + 1;
+            while (q < d[j].len && *view.at(d[j].off + q) != v) ++q;
+            if (q >= d[j].len) set_error(st, kErrInternal, 0x1d3u);
+            ix.val[slot[j]] = make_uint2(q < d[j].len ? q : kInf, e[j].y - 1u);
+        }
+        ++removed;
+    }
+    return removed;
+}
+
+__global__ void __launch_bounds__(256, 4)
+    del_index(AdjView view, RowDesc *desc, const unsigned long long *keys, Groups gr,
                           const uint32_t *list, const uint32_t *count, uint32_t *firstpos, PosIndex ix,
                           uint32_t *wide, uint32_t *wide_count, uint32_t *huge, uint32_t *huge_count,
                           unsigned long long *stats, Status *st) {
@@ -699,24 +757,29 @@ __global__ void del_index(AdjView view, RowDesc *desc, const unsigned long long 
             if (lane >= o) incl += t;
         }
         const uint32_t excl = incl - mine;
-        const uint32_t total = __shfl_sync(kFull, incl, 31);
-        for (uint32_t e0 = 0; e0 < total; e0 += 32u) {
-            const uint32_t e = e0 + lane;
-            uint32_t lo = 0, hi = 32;  // the last lane whose keys start at or before e
+        const uint32_t total = __shfl_sync(kFull, incl, 31);  // at most 32 * kLaneKeys
+        uint32_t ks[kLaneKeys];
+        bool live[kLaneKeys];
 #pragma unroll
-            for (int step = 0; step < 5; ++step) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (__shfl_sync(kFull, excl, mid) <= e)
-                    lo = mid;
-                else
-                    hi = mid;
-            }
-            const uint32_t ks = __shfl_sync(kFull, gs, lo) + (e - __shfl_sync(kFull, excl, lo));
-            if (e < total) {
-                const uint32_t u = key_src(keys[ks]);
-                removed += del_index_key(view, desc, desc[u], u, key_low(keys[ks]), firstpos + ks, ix, st);
+        for (int j = 0; j < static_cast<int>(kLaneKeys); ++j) {
+            const uint32_t e = 32u * j + lane;
+            ks[j] = 0;
+            live[j] = false;
+            if (32u * j < total) {  // warp-uniform
+                uint32_t lo = 0, hi = 32;  // the last lane whose keys start at or before e
+#pragma unroll
+                for (int step = 0; step < 5; ++step) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (__shfl_sync(kFull, excl, mid) <= e)
+                        lo = mid;
+                    else
+                        hi = mid;
+                }
+                ks[j] = __shfl_sync(kFull, gs, lo) + (e - __shfl_sync(kFull, excl, lo));
+                live[j] = e < total;
             }
         }
+        removed += del_index_keys<kLaneKeys>(view, desc, keys, ks, live, firstpos, ix, st);
         // Larger groups go to del_index_wide: up to kHugeKeys keys one warp
         // per group, more (hub rows, where uniform deletions over the edges
         // concentrate) across the whole grid in 32-key chunks.
@@ -1173,7 +1236,8 @@ __global__ void alloc_classes(ArenaAlloc *al, Status *st) {
 constexpr uint32_t kLaneAdds = 8;
 constexpr uint32_t kLaneRow = 8;
 
-__global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long *keys, Groups gr,
+__global__ void __launch_bounds__(256, 4)
+    mutate_add(AdjView view, RowDesc *desc, const unsigned long long *keys, Groups gr,
                            const unsigned long long *plan, const ArenaAlloc *al, const uint32_t *vals,
                            uint32_t *coop_list, uint32_t *coop_count, unsigned long long *stats, PosIndex ix,
                            Status *st) {
@@ -1213,8 +1277,7 @@ __global__ void mutate_add(AdjView view, RowDesc *desc, const unsigned long long
                     } else {
                         for (uint32_t j = 0; j < a; ++j) write_slot(view, d.off + d.len + j, add[j]);
                     }
-                    if (indexed)
-                        for (uint32_t j = 0; j < a; ++j) idx_add(ix, u, add[j], d.len + j, st);
+                    if (indexed) idx_add_n<kLaneAdds>(ix, u, add, d.len, a, st);
                     desc[u] = RowDesc{d.off, d.len + a, d.meta};
                     changed += 1;
                 } else if (d.len > kLaneRow) {

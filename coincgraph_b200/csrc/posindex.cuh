@@ -50,6 +50,18 @@ __device__ __forceinline__ bool idx_row(const PosIndex &ix, uint32_t v) {
     return ix.keys && ((__ldg(ix.rowbit + (v >> 5)) >> (v & 31u)) & 1u);
 }
 
+// Slot of `key`, or ~0 when absent; the probe starts at slot `s`, its
+// `first`-th step.
+__device__ __forceinline__ unsigned long long idx_find_from(const PosIndex &ix, unsigned long long key,
+                                                            unsigned long long s, uint32_t first) {
+    for (uint32_t i = first; i < kIdxProbe; ++i, s = (s + 1) & ix.mask) {
+        const unsigned long long k = *reinterpret_cast<volatile unsigned long long *>(ix.keys + s);
+        if (k == key) return s;
+        if (k == kIdxEmpty) return ~0ull;
+    }
+    return ~0ull;
+}
+
 // Slot of `key`, or ~0 when absent.
 __device__ __forceinline__ unsigned long long idx_find(const PosIndex &ix, unsigned long long key) {
     unsigned long long s = idx_mix(key) & ix.mask;
@@ -72,6 +84,36 @@ __device__ __forceinline__ unsigned long long idx_insert(const PosIndex &ix, uns
     }
     set_error(st, kErrInternal, 0x1d0u);
     return ~0ull;
+}
+
+// The first a of v[0..N) appear (again) at positions p0, p0 + 1, ... of
+// indexed row u: every key's first probe (a load, then a compare-and-swap
+// where the slot is empty) is in flight together; a collision continues
+// with idx_insert.
+template <int N>
+__device__ __forceinline__ void idx_add_n(const PosIndex &ix, uint32_t u, const uint32_t (&v)[N], uint32_t p0,
+                                          uint32_t a, Status *st) {
+    unsigned long long key[N], slot[N], seen[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        key[j] = (static_cast<unsigned long long>(u) << 32) | v[j];
+        slot[j] = idx_mix(key[j]) & ix.mask;
+        seen[j] = key[j];
+        if (static_cast<uint32_t>(j) < a)
+            seen[j] = *reinterpret_cast<volatile unsigned long long *>(ix.keys + slot[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < N; ++j)
+        if (static_cast<uint32_t>(j) < a && seen[j] == kIdxEmpty)
+            seen[j] = atomicCAS(ix.keys + slot[j], kIdxEmpty, key[j]);
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        if (static_cast<uint32_t>(j) >= a) continue;
+        if (seen[j] != kIdxEmpty && seen[j] != key[j]) slot[j] = idx_insert(ix, key[j], st);
+        if (slot[j] == ~0ull) continue;
+        atomicMin(&ix.val[slot[j]].x, p0 + j);
+        atomicAdd(&ix.val[slot[j]].y, 1u);
+    }
 }
 
 // v appears (again) at position p of indexed row u.
