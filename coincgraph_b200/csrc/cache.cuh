@@ -156,6 +156,26 @@ __global__ void seg_pick(SegTable t, uint32_t bump) {
     }
 }
 
+// One block copies one 64 KiB segment: each thread has eight 16-byte loads
+// in flight before it stores them, so a copy from host memory (about 2 us
+// away) takes two round trips instead of sixteen.
+__device__ __forceinline__ void copy_segment(uint4 *dst, const uint4 *src) {
+    constexpr uint32_t kVec = kSegEdges / 4, kDepth = 8;
+    for (uint32_t i0 = 0; i0 < kVec; i0 += kDepth * blockDim.x) {
+        uint4 r[kDepth];
+#pragma unroll
+        for (uint32_t j = 0; j < kDepth; ++j) {
+            const uint32_t i = i0 + j * blockDim.x + threadIdx.x;
+            r[j] = i < kVec ? src[i] : make_uint4(0u, 0u, 0u, 0u);
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < kDepth; ++j) {
+            const uint32_t i = i0 + j * blockDim.x + threadIdx.x;
+            if (i < kVec) dst[i] = r[j];
+        }
+    }
+}
+
 // One block per victim slot: write back if dirty, unmap, free the slot.
 __global__ void seg_evict(SegTable t, const uint32_t *cache, uint32_t *host, Status *st) {
     const uint32_t nv = min(t.ctl[kCtlEvictNeed], t.ctl[kCtlVictims]);
@@ -163,11 +183,9 @@ __global__ void seg_evict(SegTable t, const uint32_t *cache, uint32_t *host, Sta
         const uint32_t slot = t.victims[v];
         const int32_t seg = t.slot_seg[slot];
         if (seg < 0) continue;
-        if (t.seg_dirty[seg]) {
-            const uint4 *src = reinterpret_cast<const uint4 *>(cache + (static_cast<uint64_t>(slot) << kSegShift));
-            uint4 *dst = reinterpret_cast<uint4 *>(host + (static_cast<uint64_t>(seg) << kSegShift));
-            for (uint32_t i = threadIdx.x; i < kSegEdges / 4; i += blockDim.x) dst[i] = src[i];
-        }
+        if (t.seg_dirty[seg])
+            copy_segment(reinterpret_cast<uint4 *>(host + (static_cast<uint64_t>(seg) << kSegShift)),
+                         reinterpret_cast<const uint4 *>(cache + (static_cast<uint64_t>(slot) << kSegShift)));
         __syncthreads();
         if (threadIdx.x == 0) {
             __threadfence_system();
@@ -210,9 +228,8 @@ __global__ void seg_admit(SegTable t, uint32_t *cache, const uint32_t *host, Sta
         __syncthreads();
         const int32_t slot = slot_s;
         if (slot >= 0) {
-            const uint4 *src = reinterpret_cast<const uint4 *>(host + (static_cast<uint64_t>(seg) << kSegShift));
-            uint4 *dst = reinterpret_cast<uint4 *>(cache + (static_cast<uint64_t>(slot) << kSegShift));
-            for (uint32_t i = threadIdx.x; i < kSegEdges / 4; i += blockDim.x) dst[i] = src[i];
+            copy_segment(reinterpret_cast<uint4 *>(cache + (static_cast<uint64_t>(slot) << kSegShift)),
+                         reinterpret_cast<const uint4 *>(host + (static_cast<uint64_t>(seg) << kSegShift)));
             __syncthreads();
             if (threadIdx.x == 0) {
                 __threadfence();

@@ -239,17 +239,15 @@ struct DevArena {
 };
 
 // Write-back of the edge cache: copy every dirty resident segment to its
-// pinned host copy (one block per segment, 16-byte stores) and clear the flag.
+// pinned host copy (one block per segment) and clear the flag.
 __global__ void flush_dirty(uint8_t *dirty, const int32_t *seg_slot, const uint32_t *cache, uint32_t *host,
                             uint64_t nsegs) {
     for (uint64_t s = blockIdx.x; s < nsegs; s += gridDim.x) {
         if (!dirty[s]) continue;
         const int32_t slot = seg_slot[s];
-        if (slot >= 0) {
-            const uint4 *src = reinterpret_cast<const uint4 *>(cache + (static_cast<uint64_t>(slot) << kSegShift));
-            uint4 *dst = reinterpret_cast<uint4 *>(host + (s << kSegShift));
-            for (uint32_t i = threadIdx.x; i < kSegEdges / 4; i += blockDim.x) dst[i] = src[i];
-        }
+        if (slot >= 0)
+            copy_segment(reinterpret_cast<uint4 *>(host + (s << kSegShift)),
+                         reinterpret_cast<const uint4 *>(cache + (static_cast<uint64_t>(slot) << kSegShift)));
         __syncthreads();
         if (threadIdx.x == 0) dirty[s] = 0;
         __syncthreads();
