@@ -1993,6 +1993,28 @@ struct cig_handle {
         if ((nd && (!hdu || !hdv)) || (na && (!hau || !hav))) throw CigError(CIG_ERR_ARG, "null update array");
         const uint32_t *src[4] = {hdu, hdv, hau, hav};
         const uint64_t cnt[4] = {nd, nd, na, na};
+        uint32_t *dev[4] = {du, dv, au, av};
+        // Caller arrays in page-locked host memory (cudaHostAlloc,
+        // cudaHostRegister, a pinned torch tensor) are copied by DMA
+        // straight from where they are; the call ends synchronised, so they
+        // may change again once it returns.
+        bool all_pinned = true;
+        for (int a = 0; a < 4 && all_pinned; ++a) {
+            if (!cnt[a]) continue;
+            cudaPointerAttributes at{};
+            if (cudaPointerGetAttributes(&at, src[a]) != cudaSuccess) {
+                cudaGetLastError();
+                all_pinned = false;
+            } else {
+                all_pinned = at.type == cudaMemoryTypeHost;
+            }
+        }
+        if (all_pinned) {
+            for (int a = 0; a < 4; ++a)
+                if (cnt[a])
+                    CK(cudaMemcpyAsync(dev[a], src[a], cnt[a] * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+            return;
+        }
         uint32_t *dst[4] = {stage, stage + bcap, stage + 2 * bcap, stage + 3 * bcap};
         auto copy = [&](int part, int parts) {
             for (int a = 0; a < 4; ++a) {
@@ -2006,7 +2028,6 @@ struct cig_handle {
             stager_run([&](int part) { copy(part, stage_workers + 1); });
         else
             copy(0, 1);
-        uint32_t *dev[4] = {du, dv, au, av};
         for (int a = 0; a < 4; ++a)
             if (cnt[a])
                 CK(cudaMemcpyAsync(dev[a], dst[a], cnt[a] * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));

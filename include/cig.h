@@ -158,7 +158,9 @@ int cig_insert_phase(cig_handle *h, const uint32_t *u, const uint32_t *v, uint64
                      cig_batch_stats *stats);
 
 /* One whole batch: deletion phase then insertion phase (PR: UpdatePageRank,
- * framework.cuh:1660-1704).  Host arrays. */
+ * framework.cuh:1660-1704).  Host arrays: page-locked ones (cudaHostAlloc,
+ * cudaHostRegister) are copied to the device directly, pageable ones through
+ * the handle's pinned staging buffer. */
 int cig_apply_batch(cig_handle *h, const uint32_t *del_u, const uint32_t *del_v, uint64_t nd,
                     const uint32_t *add_u, const uint32_t *add_v, uint64_t na, cig_batch_stats *stats);
 
