@@ -1069,11 +1069,41 @@ __global__ void del_finish(const RowDesc *desc, const unsigned long long *keys, 
 // first positions of its keys are recomputed over the row's first `len`
 // slots at `off` (two passes, reset then minimum).  Block-wide and warp-wide
 // forms; all threads of the block (warp) call.
+// One pass over the entries t, t + stride, ... of the row: `set` false
+// clears every key's first position, true lowers it to the entry's
+// position.  Four entries per thread at a time, their row reads and index
+// probes in flight together.
+__device__ __forceinline__ void idx_reposition_pass(const AdjView &view, const PosIndex &ix, uint32_t u,
+                                                    uint64_t off, uint32_t len, uint32_t t, uint32_t stride, bool set,
+                                                    Status *st) {
+    constexpr int N = 4;
+    for (uint32_t base = t; base < len; base += N * stride) {
+        uint32_t v[N];
+        bool live[N];
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            const uint32_t k = base + j * stride;
+            live[j] = k < len;
+            v[j] = live[j] ? __ldcg(view.at(off + k)) : 0u;
+        }
+        unsigned long long slot[N];
+        idx_find_n<N>(ix, u, v, live, slot, st);
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            if (slot[j] == ~0ull) continue;
+            if (set)
+                atomicMin(&ix.val[slot[j]].x, base + j * stride);
+            else
+                atomicExch(&ix.val[slot[j]].x, kInf);
+        }
+    }
+}
+
 __device__ __forceinline__ void idx_reposition_block(const AdjView &view, const PosIndex &ix, uint32_t u,
                                                      uint64_t off, uint32_t len, Status *st) {
-    for (uint32_t k = threadIdx.x; k < len; k += blockDim.x) idx_pos_reset(ix, u, __ldcg(view.at(off + k)), st);
+    idx_reposition_pass(view, ix, u, off, len, threadIdx.x, blockDim.x, false, st);
     __syncthreads();
-    for (uint32_t k = threadIdx.x; k < len; k += blockDim.x) idx_pos_set(ix, u, __ldcg(view.at(off + k)), k);
+    idx_reposition_pass(view, ix, u, off, len, threadIdx.x, blockDim.x, true, st);
     __syncthreads();
 }
 
@@ -1081,9 +1111,9 @@ __device__ __forceinline__ void idx_reposition_warp(const AdjView &view, const P
                                                     uint64_t off, uint32_t len, Status *st) {
     const uint32_t lane = lane_id();
     __syncwarp();
-    for (uint32_t k = lane; k < len; k += 32u) idx_pos_reset(ix, u, __ldcg(view.at(off + k)), st);
+    idx_reposition_pass(view, ix, u, off, len, lane, 32u, false, st);
     __syncwarp();
-    for (uint32_t k = lane; k < len; k += 32u) idx_pos_set(ix, u, __ldcg(view.at(off + k)), k);
+    idx_reposition_pass(view, ix, u, off, len, lane, 32u, true, st);
     __syncwarp();
 }
 

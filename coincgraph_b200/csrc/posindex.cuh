@@ -86,6 +86,32 @@ __device__ __forceinline__ unsigned long long idx_insert(const PosIndex &ix, uns
     return ~0ull;
 }
 
+// The slots of the keys (u, v[j]) of an indexed row for the live j, ~0 for
+// the others: the first probe of every key is in flight together; a
+// collision continues with idx_find_from.  A live key that is absent sets
+// an internal error (the row holds it, so the index must).
+template <int N>
+__device__ __forceinline__ void idx_find_n(const PosIndex &ix, uint32_t u, const uint32_t (&v)[N],
+                                           const bool (&live)[N], unsigned long long (&slot)[N], Status *st) {
+    unsigned long long key[N], seen[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        key[j] = (static_cast<unsigned long long>(u) << 32) | v[j];
+        slot[j] = idx_mix(key[j]) & ix.mask;
+        seen[j] = key[j];
+        if (live[j]) seen[j] = *reinterpret_cast<volatile unsigned long long *>(ix.keys + slot[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        if (!live[j]) {
+            slot[j] = ~0ull;
+        } else if (seen[j] != key[j]) {
+            slot[j] = seen[j] == kIdxEmpty ? ~0ull : idx_find_from(ix, key[j], (slot[j] + 1) & ix.mask, 1);
+            if (slot[j] == ~0ull) set_error(st, kErrInternal, 0x1d1u);
+        }
+    }
+}
+
 // The first a of v[0..N) appear (again) at positions p0, p0 + 1, ... of
 // indexed row u: every key's first probe (a load, then a compare-and-swap
 // where the slot is empty) is in flight together; a collision continues
