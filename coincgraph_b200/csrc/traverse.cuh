@@ -829,14 +829,31 @@ __device__ __forceinline__ unsigned long long digest_mix(unsigned long long z) {
     return z ^ (z >> 31);
 }
 
+__device__ __forceinline__ unsigned long long value_term(uint32_t v, unsigned long long word, uint32_t ccs) {
+    const uint32_t d = val_of(word) >> ccs;
+    return d != kInf ? digest_mix((static_cast<unsigned long long>(v) << 32) | d) : 0ull;
+}
+
+// The sum is order-free, so the state is read two words per 16-byte load
+// (the array starts 16-byte aligned) and each block adds its total with one
+// atomic (one per warp queued ~10 k atomics on one address).
 __global__ void value_digest(const unsigned long long *state, uint32_t n, unsigned long long *out, uint32_t ccs) {
+    __shared__ unsigned long long part[32];
     unsigned long long acc = 0;
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-        const uint32_t d = val_of(state[v]) >> ccs;
-        if (d != kInf) acc += digest_mix((static_cast<unsigned long long>(v) << 32) | d);
+    const ulonglong2 *pairs = reinterpret_cast<const ulonglong2 *>(state);
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n / 2; p += gridDim.x * blockDim.x) {
+        const ulonglong2 w = pairs[p];
+        acc += value_term(2 * p, w.x, ccs) + value_term(2 * p + 1, w.y, ccs);
     }
+    if ((n & 1u) && blockIdx.x == 0 && threadIdx.x == 0) acc += value_term(n - 1, state[n - 1], ccs);
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
-    if (lane_id() == 0 && acc) atomicAdd(out, acc);
+    if (lane_id() == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        acc = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0ull;
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
+        if (threadIdx.x == 0 && acc) atomicAdd(out, acc);
+    }
 }
 
 }  // namespace cig

@@ -430,4 +430,18 @@ def test_pinned_host_arrays_equal_pageable():
             b.apply_batch(*(np.asarray(x, dtype=np.uint32) for x in batch))
             assert np.array_equal(a.values(), trace["batch"][i]), f"batch {i}"
             assert np.array_equal(a.values(), b.values()) and a.digest() == b.digest()
+            assert a.digest() == _value_digest(a.values())
             assert np.array_equal(a.export_csr()[1], trace["rows"][i][1])
+
+
+def _value_digest(values):
+    """cig_value_digest restated on the host: the sum mod 2^64 over reached
+    vertices v of SplitMix64((v << 32) | value)."""
+    v = np.flatnonzero(values != 0xFFFFFFFF).astype(np.uint64)
+    with np.errstate(over="ignore"):
+        z = (v << np.uint64(32)) | values[v.astype(np.int64)].astype(np.uint64)
+        z = z + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+        return int(np.sum(z, dtype=np.uint64))
