@@ -386,6 +386,50 @@ struct cig_handle {
         while (cap < 2 * (e + room)) cap <<= 1;
         return cap;
     }
+    // The initially resident segments: the small rows first (the last
+    // `small_segs` segments of the arena), then the largest classes (the
+    // first segments) while the `filled` slots last, the middle classes in
+    // host memory.  A small row costs a traversal one dependent host access
+    // per read and most reads are of small rows, while a large row crosses
+    // the link in long requests but carries the most bytes; the rows between
+    // gain the least from HBM -- as long as the position index covers them.
+    // An unindexed row is scanned whole by every deletion in it, so when the
+    // index leaves rows above the small classes out (a small --index_budget,
+    // or no index) the largest classes come first alone.
+    // CIG_CACHE_SMALL_PCT=p gives the last segments p % of the slots instead
+    // (0: the first segments only).
+    void place_resident(uint64_t filled, uint64_t small_segs) {
+        uint64_t small = 0;
+        if (refresh) {
+            if (cache_small_pct >= 0.0) {
+                small = std::min<uint64_t>(filled, static_cast<uint64_t>(filled * cache_small_pct / 100.0));
+            } else {
+                const bool middle_indexed = ixb[0].cap && ixb[0].cls <= kSmallRowClass + 1;
+                small = middle_indexed ? std::min<uint64_t>(filled, small_segs) : 0;
+            }
+        }
+        const uint64_t big = filled - small;
+        auto seg_of_slot = [&](uint64_t i) { return i < big ? i : fwd.seg_used - small + (i - big); };
+        const size_t seg_bytes = kSegEdges * sizeof(uint32_t);
+        if (big) CK(cudaMemcpy(fwd.dev, fwd.host, big * seg_bytes, cudaMemcpyHostToDevice));
+        if (small)
+            CK(cudaMemcpy(fwd.dev + big * kSegEdges, fwd.host + (fwd.seg_used - small) * kSegEdges, small * seg_bytes,
+                          cudaMemcpyHostToDevice));
+        std::vector<int32_t> slot(fwd.seg_total, -1);
+        for (uint64_t i = 0; i < resident; ++i) slot[seg_of_slot(i)] = static_cast<int32_t>(i);
+        CK(cudaMemcpy(fwd.seg_slot, slot.data(), slot.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+        if (!refresh) return;
+        std::vector<int32_t> owner(cache_slots, -1);
+        for (uint64_t i = 0; i < filled; ++i) owner[i] = static_cast<int32_t>(seg_of_slot(i));
+        std::vector<uint32_t> stack;
+        for (uint64_t k = cache_slots; k-- > filled;) stack.push_back(static_cast<uint32_t>(k));
+        CK(cudaMemcpy(slot_seg, owner.data(), cache_slots * sizeof(int32_t), cudaMemcpyHostToDevice));
+        if (!stack.empty())
+            CK(cudaMemcpy(free_slots, stack.data(), stack.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+        const uint32_t ctl[kCtlCount] = {static_cast<uint32_t>(stack.size()), static_cast<uint32_t>(fwd.seg_used)};
+        CK(cudaMemcpy(seg_ctl, ctl, sizeof(ctl), cudaMemcpyHostToDevice));
+    }
+
     void build_index(DevArena &A, bool forward) {
         IndexBuf &b = ixb[forward ? 0 : 1];
         if (!use_index) return;
@@ -1164,31 +1208,12 @@ struct cig_handle {
         refresh = cache_slots > 0 && !(opt.flags & CIG_FLAG_NO_CACHE_REFRESH);
         const uint64_t filled = std::min<uint64_t>(cache_slots, fwd.seg_used);
         resident = refresh ? filled : cache_slots;
-        // Initially resident: the small rows first (the last segments), then
-        // the largest classes (the first segments) while slots last; the
-        // middle classes start in host memory.  A small row costs a
-        // traversal one dependent host access per read and most reads are of
-        // small rows, while a large row crosses the link in long requests but
-        // carries the most bytes; the rows between gain the least from HBM.
-        // CIG_CACHE_SMALL_PCT=p instead gives the last segments p % of the
-        // slots (0: the first segments only).
-        uint64_t small = std::min<uint64_t>(filled, L.small_segs);
-        if (cache_small_pct >= 0.0)
-            small = std::min<uint64_t>(filled, static_cast<uint64_t>(filled * cache_small_pct / 100.0));
-        if (!refresh) small = 0;
-        const uint64_t big = filled - small;
-        auto seg_of_slot = [&](uint64_t i) { return i < big ? i : fwd.seg_used - small + (i - big); };
-        if (cache_slots) {
-            dmalloc(fwd.dev, cache_slots * kSegEdges);
-            const size_t seg_bytes = kSegEdges * sizeof(uint32_t);
-            if (big) CK(cudaMemcpy(fwd.dev, fwd.host, big * seg_bytes, cudaMemcpyHostToDevice));
-            if (small)
-                CK(cudaMemcpy(fwd.dev + big * kSegEdges, fwd.host + (fwd.seg_used - small) * kSegEdges,
-                              small * seg_bytes, cudaMemcpyHostToDevice));
-        }
+        if (cache_slots) dmalloc(fwd.dev, cache_slots * kSegEdges);
+        // Which segments start resident is chosen once the position index
+        // is built (place_resident); until then every segment is read from
+        // host memory (the index build reads the rows through the table).
         {
             std::vector<int32_t> slot(fwd.seg_total, -1);
-            for (uint64_t i = 0; i < resident; ++i) slot[seg_of_slot(i)] = static_cast<int32_t>(i);
             dmalloc(fwd.seg_slot, fwd.seg_total);
             CK(cudaMemcpy(fwd.seg_slot, slot.data(), slot.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
             dmalloc(fwd.seg_dirty, fwd.seg_total);
@@ -1199,22 +1224,13 @@ struct cig_handle {
         if (refresh) {
             if (const char *e = std::getenv("CIG_CACHE_ADMIT_SCORE")) admit_score = static_cast<uint32_t>(std::atol(e));
             if (const char *e = std::getenv("CIG_CACHE_COLD_SCORE")) cold_score = static_cast<uint32_t>(std::atol(e));
-            std::vector<int32_t> owner(cache_slots, -1);
-            for (uint64_t i = 0; i < filled; ++i) owner[i] = static_cast<int32_t>(seg_of_slot(i));
-            std::vector<uint32_t> stack;
-            for (uint64_t k = cache_slots; k-- > filled;) stack.push_back(static_cast<uint32_t>(k));
             dmalloc(slot_seg, cache_slots);
-            CK(cudaMemcpy(slot_seg, owner.data(), cache_slots * sizeof(int32_t), cudaMemcpyHostToDevice));
             dmalloc(free_slots, cache_slots);
-            if (!stack.empty())
-                CK(cudaMemcpy(free_slots, stack.data(), stack.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
             dmalloc(seg_score, fwd.seg_total);
             CK(cudaMemset(seg_score, 0, fwd.seg_total * sizeof(uint32_t)));
             dmalloc(seg_victims, kMaxEvict);
             dmalloc(seg_admits, kMaxAdmit);
-            const uint32_t ctl[kCtlCount] = {static_cast<uint32_t>(stack.size()), static_cast<uint32_t>(fwd.seg_used)};
             dmalloc(seg_ctl, kCtlCount);
-            CK(cudaMemcpy(seg_ctl, ctl, sizeof(ctl), cudaMemcpyHostToDevice));
         }
 
         // Reverse arena (device only) for deletion repair.
@@ -1226,6 +1242,7 @@ struct cig_handle {
         dmalloc(tmp_u32, n);
         if (local_sweeps && opt.algo != CIG_PR) dmalloc(inval_done, n + 1);
         build_index(fwd, true);
+        place_resident(filled, L.small_segs);
         if (opt.algo != CIG_PR) build_index(rev, false);
         if (opt.algo == CIG_PR) {
             const size_t es = pr64 ? sizeof(double) : sizeof(float);
