@@ -1190,7 +1190,7 @@ struct cig_handle {
         CK(cudaMemcpy(fwd.desc, L.desc.data(), n * sizeof(RowDesc), cudaMemcpyHostToDevice));
         upload_alloc(fwd, L);
 
-        // HBM edge cache: whole segments (initial choice below).
+        // HBM edge cache: whole segments (which ones start resident: place_resident).
         uint64_t budget_slots;
         if (opt.cache_compat) {
             const long long c = static_cast<long long>(opt.cache_gib);
